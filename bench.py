@@ -1,0 +1,331 @@
+#!/usr/bin/env python
+"""Benchmark of the cDTW hot path on B200 (one JSON line on rank 0).
+
+Workload (one "step"): the unpruned raw all-windows cDTW of the full-scale
+metal-like configuration -- a 2^22-sample metal-like float32 stream (cumulative
+N(0,1) increments plus N(0,20) level shifts every 1e5+-2e4 samples), a
+length-128 query cut at a seeded offset with N(0,0.1) noise, band ratios 10%
+and 20% (W = 12 and 25 by the reference's W = (int)(M*P*0.01)).  A step runs
+the windowed statistics once and the cDTW of every window for both bands.
+Metric: cell updates per second (GCUPS), cells(M,W) = M(2W+1) - W(W+1) per
+window, N-M+1 windows; stream samples/s is reported beside it.
+
+Timing: W warm-up steps, then K steps each bracketed by CUDA events on the
+launching stream, with a 256 MiB write between steps to flush the 126 MB L2
+(not timed); the whole timed region is bracketed by a barrier and
+torch.cuda.synchronize(); the job time is the max over ranks.  Weak scaling:
+each rank searches its own stream, no data-path collective.
+
+`--impl reference` times the reference's own CPU all-windows cDTW
+(openmp_cdtw, include/cdtw.cuh:91-157, restated in FP32 in the oracle because
+the header does not compile outside nvcc with its vendored CUB) on all host
+threads, on a bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_STREAM = 1 << 22
+M_QUERY = 128
+BAND_PCT = (10, 20)
+L2_FLUSH_BYTES = 256 << 20
+
+
+def cells(m: int, w: int) -> int:
+    w = min(w, m - 1)
+    return m * (2 * w + 1) - w * (w + 1)
+
+
+def workload(rank: int):
+    from cudadtw_b200 import synth
+    x = synth.metal_like(N_STREAM, seed=1 + rank)
+    q, off = synth.cut_query(x, M_QUERY, seed=1000 + rank, noise=0.1)
+    bands = [synth.band_from_percent(M_QUERY, p) for p in BAND_PCT]
+    return x, q, off, bands
+
+
+def config(bands, world: int, sample=None) -> dict:
+    c = {"workload": "raw all-windows cDTW, metal-like stream (config 1 raw part)",
+         "stream_samples": N_STREAM, "query_len": M_QUERY, "band_pct": list(BAND_PCT),
+         "bands_W": bands, "windows_per_band": N_STREAM - M_QUERY + 1,
+         "metric_cost": "squared euclidean", "parallelism": f"stream-per-rank x{world}",
+         "l2": "256 MiB write between timed steps (flush)"}
+    if sample:
+        c["sample"] = sample
+    return c
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled every 200 ms while running."""
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_id: str | None):
+        self.proc = None
+        self.path = f"/tmp/cdtw_clocks_{os.getpid()}.csv"
+        try:
+            cmd = ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                   "-lms", "200"]
+            if gpu_id:
+                cmd += ["-i", gpu_id]
+            self.proc = subprocess.Popen(cmd, stdout=open(self.path, "w"),
+                                         stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.3)
+        self.proc.terminate()
+        self.proc.wait()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [v.strip() for v in line.split(",")]
+            if len(f) < 8:
+                continue
+            try:
+                sm.append(float(f[0]))
+                mx.append(float(f[1]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[4:8]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        os.unlink(self.path)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": max(mx), "samples": len(sm),
+                "reasons": sorted(reasons)}
+
+
+def cpu_port_gcups(x, q, bands, seconds: float, seed: int = 0):
+    """The reference CPU all-windows cDTW (FP32, OpenMP, all host threads) on a
+    random sample of windows sized for about `seconds` of work."""
+    import oracle
+    zq = oracle.znorm(q).astype(np.float32)
+    threads = os.cpu_count() or 1
+    rng = np.random.default_rng(seed)
+    # stats only for the sampled windows' neighbourhood: compute on a prefix
+    span = min(x.size, 1 << 20)
+    xs = np.ascontiguousarray(x[:span])
+    mu, sd = oracle.window_stats(xs, q.size)
+    mu32, sd32 = mu.astype(np.float32), sd.astype(np.float32)
+    nw = span - q.size + 1
+    # calibrate with a small sample, then size the real one
+    probe = rng.integers(0, nw, size=2000, dtype=np.int64)
+    t0 = time.perf_counter()
+    for w in bands:
+        oracle.cdtw_ref_f32(zq, xs, mu32, sd32, probe, w, threads)
+    dt = max(time.perf_counter() - t0, 1e-3)
+    n = int(min(nw, max(2000, 2000 * seconds / dt)))
+    idx = rng.integers(0, nw, size=n, dtype=np.int64)
+    t0 = time.perf_counter()
+    for w in bands:
+        oracle.cdtw_ref_f32(zq, xs, mu32, sd32, idx, w, threads)
+    dt = time.perf_counter() - t0
+    tot_cells = sum(n * cells(q.size, w) for w in bands)
+    return tot_cells / dt / 1e9, threads, n, dt
+
+
+def run_reference(args, rank: int, world: int) -> None:
+    if rank != 0:
+        return
+    x, q, _, bands = workload(0)
+    per_step_s = max(2.0, 30.0 / max(1, args.steps + args.warmup))
+    vals, info = [], None
+    for s in range(args.warmup + args.steps):
+        g, thr, n, dt = cpu_port_gcups(x, q, bands, per_step_s, seed=s)
+        if s >= args.warmup:
+            vals.append(g)
+            info = (thr, n, dt)
+    v = float(np.median(vals))
+    thr, n, dt = info
+    sample = f"{n} random windows per band of the 2^22-sample stream (first 2^20 samples), per step"
+    line = {"impl": "reference", "metric": "GCUPS & stream samples/s", "value": v,
+            "unit": "GCUPS", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic", "config": config(bands, world, sample),
+            "stream_samples_per_s": v * 1e9 * len(bands) / sum(cells(M_QUERY, w) for w in bands),
+            "cpu_baseline": {"value": v, "unit": "GCUPS", "cores": thr, "kind": "port",
+                             "sample": sample},
+            "e2e": {"value": v, "unit": "GCUPS", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, rank: int, world: int, local_rank: int) -> None:
+    import torch
+    import torch.distributed as dist
+    from cudadtw_b200 import Handle
+    from cudadtw_b200._lib import load
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    x, q, off, bands = workload(rank)
+    nw = x.size - q.size + 1
+    cells_step = sum(nw * cells(q.size, w) for w in bands)
+
+    h = Handle(local_rank)
+    stream = torch.cuda.current_stream(dev)
+    dx = torch.from_numpy(x).to(dev)
+    dq = torch.from_numpy(q).to(dev)
+    outs = [torch.empty(nw, dtype=torch.float32, device=dev) for _ in bands]
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
+    kev = [[torch.cuda.Event(enable_timing=True) for _ in range(2)] for _ in bands]
+
+    def step(record_kernels=False):
+        avg, std = h.avg_std(dx, q.size)
+        for i, w in enumerate(bands):
+            h.set_query(dq, w)
+            if record_kernels:
+                kev[i][0].record(stream)
+            h.gpu_cdtw(dx, avg, std, out=outs[i])
+            if record_kernels:
+                kev[i][1].record(stream)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    # peak cell-update rate (issue-bound microkernel) for the roofline
+    peak = ctypes_peak(load(), h)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    smi_id = None
+    try:
+        smi_id = "GPU-" + str(torch.cuda.get_device_properties(dev).uuid)
+    except Exception:
+        pass
+    sampler = ClockSampler(smi_id)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(args.steps)]
+    kernel_ms = [[] for _ in bands]
+    for s in range(args.steps):
+        flush.fill_(s & 0xff)
+        ev[s][0].record(stream)
+        step(record_kernels=True)
+        ev[s][1].record(stream)
+        torch.cuda.synchronize()
+        for i in range(len(bands)):
+            kernel_ms[i].append(kev[i][0].elapsed_time(kev[i][1]))
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clocks = sampler.stop()
+    t_ms = sum(a.elapsed_time(b) for a, b in ev)
+    t_s = t_ms / 1e3
+    if world > 1:
+        tt = torch.tensor([t_s], dtype=torch.float64, device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_s = float(tt.item())
+    value = world * cells_step * args.steps / t_s / 1e9
+
+    # parity spot check of this run against the argmin of its own output
+    best = [int(torch.argmin(o).item()) for o in outs]
+
+    # end to end through the host-buffer C ABI call (copies inside)
+    xp = torch.from_numpy(x).pin_memory()
+    qp = q.copy()
+    hout = [torch.empty(nw, dtype=torch.float32).pin_memory() for _ in bands]
+    for i, w in enumerate(bands):  # warm
+        h.all_windows_host(qp, xp.numpy(), w, out=hout[i].numpy())
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    e_steps = max(1, min(args.steps, 5))
+    t0 = time.perf_counter()
+    for _ in range(e_steps):
+        for i, w in enumerate(bands):
+            h.all_windows_host(qp, xp.numpy(), w, out=hout[i].numpy())
+    e_s = time.perf_counter() - t0
+    if world > 1:
+        tt = torch.tensor([e_s], dtype=torch.float64, device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        e_s = float(tt.item())
+    e2e = world * cells_step * e_steps / e_s / 1e9
+
+    kern_s = [float(np.median(k)) / 1e3 for k in kernel_ms]
+    achieved = [nw * cells(q.size, w) / ks / 1e9 for w, ks in zip(bands, kern_s)]
+    ach = sum(nw * cells(q.size, w) for w in bands) / sum(kern_s) / 1e9
+
+    if rank == 0:
+        line = {"metric": "GCUPS & stream samples/s", "value": value, "unit": "GCUPS",
+                "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": t_s * 1e3 / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic (seeded metal-like stream, FP64 stats / FP32 DTW)",
+                "config": config(bands, world),
+                "stream_samples_per_s": world * nw * len(bands) * args.steps / t_s,
+                "gpu_launches": args.steps * (1 + 2 * len(bands)),
+                "clocks": clocks,
+                "e2e": {"value": e2e, "unit": "GCUPS",
+                        "h2d_bytes_per_step": len(bands) * (x.nbytes + q.nbytes),
+                        "d2h_bytes_per_step": len(bands) * nw * 4},
+                "roofline": {"bound": "alu", "kernel": "cdtw_reg_kernel",
+                             "achieved": ach, "peak": peak / 1e9, "unit": "GCUPS",
+                             "frac": ach / (peak / 1e9), "traffic": None,
+                             "per_band": {str(w): a for w, a in zip(bands, achieved)},
+                             "peak_source": "measured: cdtw_calibrate_cell_rate (FADD+FMNMX3+FFMA"
+                                            " chains) on this GPU in this run"},
+                "argmin": {str(w): b for w, b in zip(bands, best)}, "cut_offset": off}
+        if world == 1:
+            g, thr, n, dt = cpu_port_gcups(x, q, bands, 10.0)
+            line["cpu_baseline"] = {
+                "value": g, "unit": "GCUPS", "cores": thr, "kind": "port",
+                "sample": f"{n} random windows per band (first 2^20 samples), FP32 OpenMP "
+                          f"restatement of openmp_cdtw, {dt:.1f}s"}
+        print(json.dumps(line), flush=True)
+    h.close()
+
+
+def ctypes_peak(lib, h) -> float:
+    import ctypes
+    v = ctypes.c_double()
+    st = lib.cdtw_calibrate_cell_rate(h._h, ctypes.byref(v))
+    if st != 0:
+        raise RuntimeError(lib.cdtw_last_error(h._h).decode())
+    return v.value
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    try:
+        run_ours(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

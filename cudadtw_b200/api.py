@@ -1,0 +1,155 @@
+"""Host-side mirror of the reference's search interface over the C ABI.
+
+The reference exposes header templates taking device pointers
+(avg_std<prefx_t>(Series, AvgS, StdS, M, N, stream), include/stats.cuh:115;
+gpu_cdtw<euclidean>(Subject, AvgS, StdS, Cdtw, M, Indices, L, W, ...),
+include/cdtw.cuh:450; prune_cdtw<euclidean>(Subject, AvgS, StdS, M, N, W),
+cdtw.cuh:510) with the query in __constant__ memory.  ``Handle`` keeps the
+same names and argument meaning with torch CUDA tensors as device buffers and
+the query as per-handle state.  Errors raise ``CudaDTWError`` carrying the C
+status; nothing falls back to the CPU.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+import torch
+
+from ._lib import CudaDTWError, load
+
+EUCLIDEAN, MANHATTAN = 0, 1
+HOST, DEVICE = 0, 1
+
+
+def _metric(m) -> int:
+    if m in (EUCLIDEAN, "euclidean", True):
+        return EUCLIDEAN
+    if m in (MANHATTAN, "manhattan", False):
+        return MANHATTAN
+    raise ValueError(f"unknown metric {m!r}")
+
+
+def band_from_percent(m: int, p: int) -> int:
+    """W = M*(P*0.01) truncated (GPU-dtw.cu:27)."""
+    return load().cdtw_band_from_percent(m, p)
+
+
+def _ptr(t) -> ctypes.c_void_p:
+    if t is None:
+        return ctypes.c_void_p(0)
+    if isinstance(t, np.ndarray):
+        return ctypes.c_void_p(t.ctypes.data)
+    return ctypes.c_void_p(t.data_ptr())
+
+
+def _dev(t: torch.Tensor, dtype: torch.dtype, name: str) -> torch.Tensor:
+    if not isinstance(t, torch.Tensor) or not t.is_cuda:
+        raise TypeError(f"{name} must be a CUDA tensor")
+    if t.dtype != dtype or not t.is_contiguous():
+        raise TypeError(f"{name} must be a contiguous {dtype} tensor")
+    return t
+
+
+class Handle:
+    """One cudadtw handle: device, stream, query state and work buffers."""
+
+    def __init__(self, device: int = 0):
+        self._lib = load()
+        h = ctypes.c_void_p()
+        st = self._lib.cdtw_create(ctypes.byref(h), device)
+        if st != 0:
+            raise CudaDTWError(st, f"cdtw_create(device={device}) failed: "
+                                   f"{self._lib.cdtw_status_string(st).decode()}")
+        self._h = h
+        self.device = device
+        self.M = None
+        self.W = None
+        # Work on torch's current stream so torch-made inputs are ordered
+        # before the kernels and torch consumers after them.
+        self.use_torch_stream()
+
+    # -- plumbing ----------------------------------------------------------
+    def _check(self, st: int) -> None:
+        if st != 0:
+            raise CudaDTWError(st, self._lib.cdtw_last_error(self._h).decode())
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            self._lib.cdtw_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def use_torch_stream(self, stream: torch.cuda.Stream | None = None) -> None:
+        """Run on a torch stream (default: torch's current stream)."""
+        s = stream if stream is not None else torch.cuda.current_stream(self.device)
+        self._check(self._lib.cdtw_set_stream(self._h, ctypes.c_void_p(s.cuda_stream)))
+
+    # -- reference-named operations -----------------------------------------
+    def avg_std(self, series: torch.Tensor, M: int):
+        """Windowed mean (FP64) and std (FP32) of every length-M window
+        (avg_std, include/stats.cuh:115-142)."""
+        _dev(series, torch.float32, "series")
+        nw = series.numel() - M + 1
+        avg = torch.empty(max(nw, 0), dtype=torch.float64, device=series.device)
+        std = torch.empty(max(nw, 0), dtype=torch.float32, device=series.device)
+        self._check(self._lib.cdtw_avg_std(self._h, _ptr(series), series.numel(), M, _ptr(avg),
+                                           _ptr(std)))
+        return avg, std
+
+    def set_query(self, query, W: int) -> None:
+        """z-normalise the query and build its envelope (znormalize + envelope +
+        cudaMemcpyToSymbol of GPU-dtw.cu:67-68, :82-84)."""
+        if isinstance(query, torch.Tensor) and query.is_cuda:
+            keep, loc, n = _dev(query, torch.float32, "query"), DEVICE, query.numel()
+        else:
+            keep = np.ascontiguousarray(np.asarray(query, dtype=np.float32))
+            loc, n = HOST, keep.size
+        self._check(self._lib.cdtw_set_query(self._h, _ptr(keep), n, W, loc))
+        self.M = n
+        self.W = min(W, self.M - 1)
+
+    def gpu_cdtw(self, subject: torch.Tensor, avg: torch.Tensor, std: torch.Tensor,
+                 indices: torch.Tensor | None = None, metric=EUCLIDEAN,
+                 out: torch.Tensor | None = None) -> torch.Tensor:
+        """cDTW of the query against listed windows, all windows if ``indices``
+        is None (gpu_cdtw, include/cdtw.cuh:450-487).  Squared distances for
+        the Euclidean cost, as the reference's Cdtw array."""
+        _dev(subject, torch.float32, "subject")
+        _dev(avg, torch.float64, "avg")
+        _dev(std, torch.float32, "std")
+        if indices is not None:
+            _dev(indices, torch.int32, "indices")
+            n = indices.numel()
+        else:
+            n = subject.numel() - self.M + 1
+        if out is None:
+            out = torch.empty(n, dtype=torch.float32, device=subject.device)
+        self._check(self._lib.cdtw_gpu_cdtw(self._h, _ptr(subject), subject.numel(), _ptr(avg),
+                                            _ptr(std), _ptr(indices), n, _metric(metric),
+                                            _ptr(out)))
+        return out
+
+    def all_windows_host(self, query: np.ndarray, subject: np.ndarray, W: int,
+                         metric=EUCLIDEAN, out: np.ndarray | None = None) -> np.ndarray:
+        """Unpruned all-windows cDTW from host arrays (copies inside the call)."""
+        q = np.ascontiguousarray(query, dtype=np.float32)
+        s = subject if (isinstance(subject, np.ndarray) and subject.dtype == np.float32
+                        and subject.flags.c_contiguous) else np.ascontiguousarray(subject, np.float32)
+        nw = s.size - q.size + 1
+        if out is None:
+            out = np.empty(nw, np.float32)
+        self._check(self._lib.cdtw_all_windows_host(self._h, _ptr(q), q.size, _ptr(s), s.size, W,
+                                                    _metric(metric), _ptr(out)))
+        return out

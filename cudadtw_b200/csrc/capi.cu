@@ -1,0 +1,238 @@
+// C ABI entry points (include/cudadtw.h): handle lifecycle, argument checks,
+// workspace management, and the host-buffer convenience calls.
+#include "common.cuh"
+
+#include <new>
+
+namespace cdtw {
+
+int set_error(cdtw_handle h, int status, const char* fmt, ...) {
+    if (h) {
+        va_list ap;
+        va_start(ap, fmt);
+        vsnprintf(h->err, sizeof(h->err), fmt, ap);
+        va_end(ap);
+    }
+    return status;
+}
+
+int check_cuda(cdtw_handle h, cudaError_t e, const char* what) {
+    if (e == cudaSuccess) return CDTW_OK;
+    if (e == cudaErrorMemoryAllocation) {
+        cudaGetLastError();
+        return set_error(h, CDTW_ENOMEM, "%s: %s", what, cudaGetErrorString(e));
+    }
+    return set_error(h, CDTW_ECUDA, "%s: %s", what, cudaGetErrorString(e));
+}
+
+int ensure_workspace(cdtw_handle h, size_t bytes) {
+    if (bytes <= h->ws_bytes) return CDTW_OK;
+    if (h->ws) {
+        // the old block may still be in use by queued work on the stream
+        CDTW_CUDA(h, cudaStreamSynchronize(h->stream));
+        CDTW_CUDA(h, cudaFree(h->ws));
+        h->ws = nullptr;
+        h->ws_bytes = 0;
+    }
+    const size_t want = round_up((int64_t)bytes, 1 << 20);
+    CDTW_CUDA(h, cudaMalloc(&h->ws, want));
+    h->ws_bytes = want;
+    return CDTW_OK;
+}
+
+// Sub-allocation of the workspace: 256-byte aligned slices.
+struct Carver {
+    size_t off = 0;
+    template <class T>
+    size_t take(size_t count) {
+        const size_t o = off;
+        off = (size_t)round_up((int64_t)(off + count * sizeof(T)), 256);
+        return o;
+    }
+};
+
+static int ensure_query_mem(cdtw_handle h, int M, int W) {
+    QueryPack& q = h->q;
+    const int lq = (int)round_up(M + 2 * W + 8, 4);
+    Carver c;
+    const size_t o_qpad = c.take<float>(4 * (size_t)lq);
+    const size_t o_env = c.take<float2>(M);
+    const size_t o_zq = c.take<float>(M);
+    const size_t o_zq64 = c.take<double>(M);
+    const size_t bytes = c.off;
+    if (bytes > h->qmem_bytes) {
+        if (h->qmem) {
+            CDTW_CUDA(h, cudaStreamSynchronize(h->stream));
+            CDTW_CUDA(h, cudaFree(h->qmem));
+            h->qmem = nullptr;
+            h->qmem_bytes = 0;
+        }
+        CDTW_CUDA(h, cudaMalloc(&h->qmem, bytes));
+        h->qmem_bytes = bytes;
+    }
+    char* base = (char*)h->qmem;
+    q.M = M;
+    q.W = W;
+    q.lq = lq;
+    q.qpad = (float*)(base + o_qpad);
+    q.env = (float2*)(base + o_env);
+    q.zq = (float*)(base + o_zq);
+    q.zq64 = (double*)(base + o_zq64);
+    return CDTW_OK;
+}
+
+static bool valid_metric(int metric) { return metric == CDTW_EUCLIDEAN || metric == CDTW_MANHATTAN; }
+
+}  // namespace cdtw
+
+using namespace cdtw;
+
+extern "C" {
+
+int cdtw_create(cdtw_handle* out, int device) {
+    if (!out) return CDTW_EINVAL;
+    *out = nullptr;
+    int ndev = 0;
+    cudaError_t e = cudaGetDeviceCount(&ndev);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return CDTW_ECUDA;
+    }
+    if (device < 0 || device >= ndev) return CDTW_EINVAL;
+    cdtw_handle h = new (std::nothrow) cdtw_handle_s();
+    if (!h) return CDTW_ENOMEM;
+    h->device = device;
+    if (cudaSetDevice(device) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaDeviceGetAttribute(&h->sm_count, cudaDevAttrMultiProcessorCount, device) !=
+            cudaSuccess ||
+        cudaMallocHost(&h->pinned, 4096) != cudaSuccess) {
+        cudaGetLastError();
+        if (h->own_stream) cudaStreamDestroy(h->own_stream);
+        delete h;
+        return CDTW_ECUDA;
+    }
+    h->stream = h->own_stream;
+    *out = h;
+    return CDTW_OK;
+}
+
+int cdtw_destroy(cdtw_handle h) {
+    if (!h) return CDTW_EINVAL;
+    cudaSetDevice(h->device);
+    cudaStreamSynchronize(h->stream);
+    if (h->ws) cudaFree(h->ws);
+    if (h->qmem) cudaFree(h->qmem);
+    if (h->pinned) cudaFreeHost(h->pinned);
+    if (h->own_stream) cudaStreamDestroy(h->own_stream);
+    delete h;
+    return CDTW_OK;
+}
+
+int cdtw_set_stream(cdtw_handle h, void* cuda_stream) {
+    if (!h) return CDTW_EINVAL;
+    h->stream = cuda_stream ? (cudaStream_t)cuda_stream : h->own_stream;
+    return CDTW_OK;
+}
+
+const char* cdtw_last_error(cdtw_handle h) { return h ? h->err : "null handle"; }
+
+const char* cdtw_status_string(int status) {
+    switch (status) {
+        case CDTW_OK: return "ok";
+        case CDTW_EINVAL: return "invalid argument";
+        case CDTW_ENOMEM: return "out of memory";
+        case CDTW_ECUDA: return "CUDA error";
+        case CDTW_ETIMEOUT: return "device wait timed out";
+        case CDTW_EUNSUPPORTED: return "unsupported";
+        default: return "unknown status";
+    }
+}
+
+int cdtw_band_from_percent(int M, int P) { return (int)(M * (P * 0.01)); }
+
+int cdtw_avg_std(cdtw_handle h, const float* d_series, int64_t N, int M, double* d_avg,
+                 float* d_std) {
+    if (!h) return CDTW_EINVAL;
+    if (!d_series || !d_avg || !d_std) return set_error(h, CDTW_EINVAL, "null pointer");
+    if (M < 1 || N < M) return set_error(h, CDTW_EINVAL, "need 1 <= M <= N (M=%d N=%lld)", M,
+                                         (long long)N);
+    if (N - M + 1 > INT32_MAX) return set_error(h, CDTW_EUNSUPPORTED, "too many windows");
+    CDTW_CUDA(h, cudaSetDevice(h->device));
+    return launch_avg_std(h, d_series, N, M, d_avg, d_std);
+}
+
+int cdtw_set_query(cdtw_handle h, const float* query, int M, int W, int query_loc) {
+    if (!h) return CDTW_EINVAL;
+    if (!query) return set_error(h, CDTW_EINVAL, "null query");
+    if (M < 1 || M > CDTW_MAX_QUERY)
+        return set_error(h, CDTW_EINVAL, "query length %d outside [1, %d]", M, CDTW_MAX_QUERY);
+    if (W < 0) return set_error(h, CDTW_EINVAL, "negative band %d", W);
+    if (query_loc != CDTW_HOST && query_loc != CDTW_DEVICE)
+        return set_error(h, CDTW_EINVAL, "bad query location %d", query_loc);
+    if (W > M - 1) W = M - 1;  // a wider band changes nothing
+    CDTW_CUDA(h, cudaSetDevice(h->device));
+    CDTW_TRY(ensure_query_mem(h, M, W));
+    const float* dq = query;
+    if (query_loc == CDTW_HOST) {
+        // stage the raw query in the (now unused) zq slot of the pack
+        CDTW_CUDA(h, cudaMemcpyAsync(h->q.zq, query, sizeof(float) * M, cudaMemcpyHostToDevice,
+                                     h->stream));
+        dq = h->q.zq;
+    }
+    CDTW_TRY(launch_prepare_query(h, dq, M, W));
+    h->has_query = true;
+    return CDTW_OK;
+}
+
+int cdtw_gpu_cdtw(cdtw_handle h, const float* d_subject, int64_t N, const double* d_avg,
+                  const float* d_std, const int32_t* d_indices, int64_t L, int metric,
+                  float* d_out) {
+    if (!h) return CDTW_EINVAL;
+    if (!h->has_query) return set_error(h, CDTW_EINVAL, "no query set (cdtw_set_query)");
+    if (!d_subject || !d_avg || !d_std || !d_out)
+        return set_error(h, CDTW_EINVAL, "null pointer");
+    if (!valid_metric(metric)) return set_error(h, CDTW_EINVAL, "bad metric %d", metric);
+    const int M = h->q.M;
+    if (N < M) return set_error(h, CDTW_EINVAL, "subject shorter than query");
+    const int64_t Nw = N - M + 1;
+    if (!d_indices) L = Nw;
+    if (L < 0 || L > INT32_MAX) return set_error(h, CDTW_EINVAL, "bad index count");
+    CDTW_CUDA(h, cudaSetDevice(h->device));
+    return launch_cdtw_windows(h, d_subject, N, d_avg, d_std, d_indices, L,
+                               metric == CDTW_EUCLIDEAN, d_out);
+}
+
+int cdtw_all_windows_host(cdtw_handle h, const float* h_query, int M, const float* h_subject,
+                          int64_t N, int W, int metric, float* h_out) {
+    if (!h) return CDTW_EINVAL;
+    if (!h_query || !h_subject || !h_out) return set_error(h, CDTW_EINVAL, "null pointer");
+    if (!valid_metric(metric)) return set_error(h, CDTW_EINVAL, "bad metric %d", metric);
+    if (M < 1 || N < M) return set_error(h, CDTW_EINVAL, "need 1 <= M <= N");
+    const int64_t Nw = N - M + 1;
+    if (Nw > INT32_MAX) return set_error(h, CDTW_EUNSUPPORTED, "too many windows");
+    CDTW_CUDA(h, cudaSetDevice(h->device));
+    Carver c;
+    const size_t o_x = c.take<float>(N);
+    const size_t o_mu = c.take<double>(Nw);
+    const size_t o_sd = c.take<float>(Nw);
+    const size_t o_out = c.take<float>(Nw);
+    CDTW_TRY(ensure_workspace(h, c.off));
+    char* base = (char*)h->ws;
+    float* dx = (float*)(base + o_x);
+    double* dmu = (double*)(base + o_mu);
+    float* dsd = (float*)(base + o_sd);
+    float* dout = (float*)(base + o_out);
+    CDTW_CUDA(h, cudaMemcpyAsync(dx, h_subject, sizeof(float) * N, cudaMemcpyHostToDevice,
+                                 h->stream));
+    CDTW_TRY(cdtw_set_query(h, h_query, M, W, CDTW_HOST));
+    CDTW_TRY(launch_avg_std(h, dx, N, M, dmu, dsd));
+    CDTW_TRY(launch_cdtw_windows(h, dx, N, dmu, dsd, nullptr, Nw, metric == CDTW_EUCLIDEAN,
+                                 dout));
+    CDTW_CUDA(h, cudaMemcpyAsync(h_out, dout, sizeof(float) * Nw, cudaMemcpyDeviceToHost,
+                                 h->stream));
+    CDTW_CUDA(h, cudaStreamSynchronize(h->stream));
+    return CDTW_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,135 @@
+// Banded DTW with the whole band of one window in registers ("register band").
+//
+// Reference: sparse_block_cdtw / dense_block_cdtw (include/cdtw.cuh:164-363),
+// which spread one window over W+2 threads and step the anti-diagonals through
+// shared memory with a __syncthreads per step.  Windows are independent and
+// there are millions of them, so here one thread owns one window and keeps
+// the 2W+1 band cells of the current row in registers; the 32 lanes of a warp
+// run 32 neighbouring windows in lockstep, so all lanes read the same query
+// values (a shared-memory broadcast) and consecutive stream samples (one
+// coalesced 128-byte load per row).
+//
+// Orientation: rows are window (data) positions j = 0..M-1, columns are query
+// positions i, band coordinate k = i - j + W in [0, 2W].  The cell update
+//   D[j][k] = cost(z_j, q_{j-W+k}) + min(D[j-1][k], D[j-1][k+1], D[j][k-1])
+// is one FADD, one three-input FMNMX and one FFMA.  Query positions outside
+// [0, M) are padded with +inf, which makes out-of-matrix cells +inf without
+// any per-cell test.  The result D[M-1][W] equals the reference's
+// penalty[...][M] (cdtw.cuh:83).
+#include "common.cuh"
+
+namespace cdtw {
+
+namespace {
+
+constexpr int kRegBlock = 128;
+constexpr int kMaxRegW = 40;
+
+template <int W, bool EU>
+__global__ void __launch_bounds__(kRegBlock)
+cdtw_reg_kernel(const float* __restrict__ x, const double* __restrict__ mu,
+                const float* __restrict__ sigma, const float4* __restrict__ qpad4, int lq4,
+                int M, const int32_t* __restrict__ idx, int L, float* __restrict__ out) {
+    extern __shared__ float4 sq4[];
+    for (int e = threadIdx.x; e < 4 * lq4; e += blockDim.x) sq4[e] = qpad4[e];
+    __syncthreads();
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= L) return;
+    const int w = idx ? idx[t] : t;
+    const Norm nm = make_norm(mu[w], sigma[w]);
+    const float* __restrict__ xw = x + w;
+
+    constexpr int B = 2 * W + 1;
+    constexpr int NQ4 = (B + 3) / 4;
+    float prev[B + 1];
+#pragma unroll
+    for (int k = 0; k <= B; ++k) prev[k] = CDTW_INF;
+    prev[W] = 0.0f;  // virtual D[-1][-1] = 0 (cdtw.cuh:35, :191)
+    float res = CDTW_INF;
+
+    for (int j0 = 0; j0 < M; j0 += 4) {
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int j = j0 + u;
+            const float z = znorm(nm, __ldg(xw + min(j, M - 1)));
+            const float4* qr = sq4 + u * lq4 + (j0 >> 2);
+            float qv[NQ4 * 4];
+#pragma unroll
+            for (int r = 0; r < NQ4; ++r) {
+                const float4 v = qr[r];
+                qv[4 * r + 0] = v.x;
+                qv[4 * r + 1] = v.y;
+                qv[4 * r + 2] = v.z;
+                qv[4 * r + 3] = v.w;
+            }
+            float left = CDTW_INF;
+            float cur[B];
+#pragma unroll
+            for (int k = 0; k < B; ++k) {
+                const float m = min3f(prev[k], prev[k + 1], left);
+                left = cell<EU>(z - qv[k], m);
+                cur[k] = left;
+            }
+            if (j == M - 1) res = cur[W];
+#pragma unroll
+            for (int k = 0; k < B; ++k) prev[k] = cur[k];
+        }
+    }
+    out[t] = res;
+}
+
+using RegKernel = void (*)(const float*, const double*, const float*, const float4*, int, int,
+                           const int32_t*, int, float*);
+
+template <int W>
+struct RegTable {
+    static void fill(RegKernel* eu, RegKernel* mh) {
+        eu[W] = cdtw_reg_kernel<W, true>;
+        mh[W] = cdtw_reg_kernel<W, false>;
+        RegTable<W - 1>::fill(eu, mh);
+    }
+};
+template <>
+struct RegTable<-1> {
+    static void fill(RegKernel*, RegKernel*) {}
+};
+
+struct RegKernels {
+    RegKernel eu[kMaxRegW + 1];
+    RegKernel mh[kMaxRegW + 1];
+    RegKernels() { RegTable<kMaxRegW>::fill(eu, mh); }
+};
+
+const RegKernels& reg_kernels() {
+    static RegKernels k;
+    return k;
+}
+
+}  // namespace
+
+int max_register_band() { return kMaxRegW; }
+
+int launch_cdtw_windows(cdtw_handle h, const float* x, int64_t N, const double* mu,
+                        const float* sigma, const int32_t* idx, int64_t L, bool euclid,
+                        float* out) {
+    (void)N;
+    const QueryPack& q = h->q;
+    if (q.W > kMaxRegW)
+        return set_error(h, CDTW_EUNSUPPORTED, "band W=%d above the register-band limit %d", q.W,
+                         kMaxRegW);
+    if (L <= 0) return CDTW_OK;
+    RegKernel k = euclid ? reg_kernels().eu[q.W] : reg_kernels().mh[q.W];
+    const int lq4 = q.lq / 4;
+    const size_t smem = (size_t)q.lq * 4 * sizeof(float);
+    if (smem > 48 * 1024)
+        CDTW_CUDA(h, cudaFuncSetAttribute((const void*)k,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)smem));
+    const unsigned blocks = (unsigned)div_up(L, kRegBlock);
+    k<<<blocks, kRegBlock, smem, h->stream>>>(x, mu, sigma, (const float4*)q.qpad, lq4, q.M, idx,
+                                              (int)L, out);
+    CDTW_LAUNCH(h, "cdtw_reg_kernel");
+    return CDTW_OK;
+}
+
+}  // namespace cdtw

@@ -1,0 +1,134 @@
+// Internal definitions shared by the sm_100a kernels and the C ABI.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stdio.h>
+#include <stdarg.h>
+#include <math.h>
+#include <string.h>
+
+#include "../../include/cudadtw.h"
+
+#define CDTW_INF __int_as_float(0x7f800000)
+
+namespace cdtw {
+
+// ---- per-handle state ------------------------------------------------------
+
+// Device layout of the prepared query ("query pack").  The reference keeps the
+// z-normalised query and its envelope in __constant__ arrays
+// (include/cdtw.cuh:9-11); here they live in one handle-owned device block:
+//   qpad  : 4 shifted copies of the +inf-padded query, copy m holds
+//           qp[a+m] where qp[a] = zq[a-W] (zq outside [0,M) = +inf).  Row j of
+//           the register-band kernel reads qp[j..j+2W] with 16-byte loads from
+//           copy (j&3) at index (j&~3).
+//   env   : (L_k, U_k) pairs of the query envelope over +-W.
+//   zq    : z-normalised query (float).
+struct QueryPack {
+    int M = 0, W = 0;
+    int lq = 0;            // floats per qpad copy (multiple of 4)
+    float* qpad = nullptr; // 4 * lq floats
+    float2* env = nullptr; // M pairs
+    float* zq = nullptr;   // M floats
+    double* zq64 = nullptr;// M doubles
+};
+
+}  // namespace cdtw
+
+struct cdtw_handle_s {
+    int device = 0;
+    int sm_count = 148;
+    cudaStream_t stream = nullptr;
+    cudaStream_t own_stream = nullptr;
+    // grow-only device workspace
+    void* ws = nullptr;
+    size_t ws_bytes = 0;
+    // query pack storage (grow-only)
+    void* qmem = nullptr;
+    size_t qmem_bytes = 0;
+    cdtw::QueryPack q;
+    bool has_query = false;
+    // small pinned host buffer for scalar results
+    void* pinned = nullptr;
+    char err[512] = {0};
+};
+
+namespace cdtw {
+
+int set_error(cdtw_handle h, int status, const char* fmt, ...);
+int check_cuda(cdtw_handle h, cudaError_t e, const char* what);
+int ensure_workspace(cdtw_handle h, size_t bytes);
+
+#define CDTW_TRY(expr)                        \
+    do {                                      \
+        int _st = (expr);                     \
+        if (_st != CDTW_OK) return _st;       \
+    } while (0)
+
+#define CDTW_CUDA(h, call) CDTW_TRY(::cdtw::check_cuda((h), (call), #call))
+#define CDTW_LAUNCH(h, what) CDTW_TRY(::cdtw::check_cuda((h), cudaGetLastError(), (what)))
+
+__host__ __device__ inline int64_t div_up(int64_t a, int64_t b) { return (a + b - 1) / b; }
+__host__ __device__ inline int64_t round_up(int64_t a, int64_t b) { return div_up(a, b) * b; }
+
+// Three-input minimum (PTX ISA 8.8, sm_100+): one instruction for the three
+// DTW predecessors.  NaN-ignoring like fminf.
+__device__ __forceinline__ float min3f(float a, float b, float c) {
+    float r;
+    asm("min.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+    return r;
+}
+__device__ __forceinline__ float max3f(float a, float b, float c) {
+    float r;
+    asm("max.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+    return r;
+}
+
+// Cell cost of the reference kernels: (z-q)^2 or |z-q| (cdtw.cuh:235-240).
+template <bool EUCLID>
+__device__ __forceinline__ float cell(float d, float m) {
+    return EUCLID ? fmaf(d, d, m) : fabsf(d) + m;
+}
+
+// Per-window normalisation constants from FP64 mean / FP32 sigma:
+// z = (x - mu_hi) * s + c with mu = mu_hi + mu_lo (double-float) and
+// c = -mu_lo * s.  x - mu_hi is exact up to one rounding of the (small)
+// difference, so level-shifted windows keep full FP32 precision in z.
+struct Norm {
+    float mhi, s, c;
+};
+__device__ __forceinline__ Norm make_norm(double mu, float sigma) {
+    Norm n;
+    n.mhi = (float)mu;
+    const float mlo = (float)(mu - (double)n.mhi);
+    n.s = 1.0f / sigma;
+    n.c = -mlo * n.s;
+    return n;
+}
+__device__ __forceinline__ float znorm(const Norm& n, float x) {
+    return fmaf(x - n.mhi, n.s, n.c);
+}
+
+// Packed (distance, index) key for the fused argmin: distances are >= 0 so
+// their float bits order like unsigned ints; ties keep the lowest index
+// (UCR's first strict minimum, UCR_DTW_BIN.cpp:682).
+__host__ __device__ inline unsigned long long pack_key(float d, uint32_t idx) {
+#ifdef __CUDA_ARCH__
+    return ((unsigned long long)__float_as_uint(d) << 32) | idx;
+#else
+    uint32_t b;
+    memcpy(&b, &d, 4);
+    return ((unsigned long long)b << 32) | idx;
+#endif
+}
+
+// ---- kernel launchers (defined in the .cu files) ----------------------------
+
+int launch_avg_std(cdtw_handle h, const float* x, int64_t N, int M, double* mu, float* sigma);
+int launch_prepare_query(cdtw_handle h, const float* d_query_raw, int M, int W);
+int launch_cdtw_windows(cdtw_handle h, const float* x, int64_t N, const double* mu,
+                        const float* sigma, const int32_t* idx, int64_t L, bool euclid,
+                        float* out);
+
+}  // namespace cdtw

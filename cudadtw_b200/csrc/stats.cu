@@ -1,0 +1,160 @@
+// Windowed statistics of the stream and preparation of the query.
+//
+// Reference: include/stats.cuh.  The reference makes two FP64 prefix sums over
+// the whole stream (CUB scans, 2 cudaMalloc + 5 kernels per 1e7-sample epoch,
+// stats.cuh:85-142) and then takes the variance in FP32 (stats.cuh:49), which
+// loses the variance of level-shifted signals.  Here one kernel reads the
+// stream once: each warp owns a run of consecutive windows, keeps FP64 sums
+// of (x-c) and (x-c)^2 for a warp-local shift c, and slides them 32 windows
+// per round with a warp scan of the entering-minus-leaving terms.  Output per
+// window: mean (FP64) and sigma (FP32), 12 bytes.
+#include "common.cuh"
+
+namespace cdtw {
+
+namespace {
+
+constexpr int kStatsRounds = 64;                 // rounds of 32 windows per warp
+constexpr int kStatsWarpWindows = 32 * kStatsRounds;
+constexpr int kStatsBlock = 128;                 // 4 warps per block
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+__device__ __forceinline__ double warp_incl_scan(double v, int lane) {
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const double t = __shfl_up_sync(0xffffffffu, v, o);
+        if (lane >= o) v += t;
+    }
+    return v;
+}
+
+__global__ void __launch_bounds__(kStatsBlock)
+avg_std_kernel(const float* __restrict__ x, int64_t N, int M, double* __restrict__ mu,
+               float* __restrict__ sigma) {
+    const int64_t Nw = N - M + 1;
+    const int lane = threadIdx.x & 31;
+    const int64_t warp = (int64_t)blockIdx.x * (kStatsBlock / 32) + (threadIdx.x >> 5);
+    const int64_t a = warp * kStatsWarpWindows;
+    if (a >= Nw) return;
+    const double c = (double)x[a];
+    // sums of the first window of the run
+    double s1 = 0.0, s2 = 0.0;
+    for (int k = lane; k < M; k += 32) {
+        const double v = (double)x[a + k] - c;
+        s1 += v;
+        s2 = fma(v, v, s2);
+    }
+    s1 = warp_sum(s1);
+    s2 = warp_sum(s2);
+    const double invM = 1.0 / (double)M;
+    for (int r = 0; r < kStatsRounds; ++r) {
+        const int64_t w = a + (int64_t)r * 32 + lane;
+        if (a + (int64_t)r * 32 >= Nw) break;  // warp-uniform
+        double d1 = 0.0, d2 = 0.0;
+        if (w < Nw - 1) {
+            // window w+1 = window w + x[w+M] - x[w]
+            const double vin = (double)x[w + M] - c, vout = (double)x[w] - c;
+            d1 = vin - vout;
+            d2 = vin * vin - vout * vout;
+        }
+        const double i1 = warp_incl_scan(d1, lane), i2 = warp_incl_scan(d2, lane);
+        // sums of window w: base + exclusive scan
+        const double w1 = s1 + (i1 - d1), w2 = s2 + (i2 - d2);
+        if (w < Nw) {
+            const double m1 = w1 * invM;
+            const double var = w2 * invM - m1 * m1;
+            mu[w] = c + m1;
+            sigma[w] = var > 0.0 ? (float)sqrt(var) : 1.0f;
+        }
+        s1 += __shfl_sync(0xffffffffu, i1, 31);
+        s2 += __shfl_sync(0xffffffffu, i2, 31);
+    }
+}
+
+// One block prepares the query pack: FP64 two-pass z-normalisation (the
+// reference does this on the host in FP32, GPU-dtw.cu:67 / stats.cuh:8-28),
+// the +inf-padded shifted copies read by the cDTW kernels, and the +-W
+// envelope (same values as Lemire's filter, bounds.cuh:13-64).
+__global__ void __launch_bounds__(256)
+prepare_query_kernel(const float* __restrict__ qraw, int M, int W, QueryPack p) {
+    __shared__ double red[2][8];
+    extern __shared__ double zs[];  // M doubles
+    const int t = threadIdx.x, lane = t & 31, wid = t >> 5;
+    double s = 0.0;
+    for (int i = t; i < M; i += blockDim.x) {
+        const double v = (double)qraw[i];
+        zs[i] = v;
+        s += v;
+    }
+    s = warp_sum(s);
+    if (lane == 0) red[0][wid] = s;
+    __syncthreads();
+    double tot = 0.0;
+    for (int k = 0; k < (int)(blockDim.x >> 5); ++k) tot += red[0][k];
+    const double mean = tot / M;
+    double v2 = 0.0;
+    for (int i = t; i < M; i += blockDim.x) {
+        const double d = zs[i] - mean;
+        v2 = fma(d, d, v2);
+    }
+    v2 = warp_sum(v2);
+    if (lane == 0) red[1][wid] = v2;
+    __syncthreads();
+    double vt = 0.0;
+    for (int k = 0; k < (int)(blockDim.x >> 5); ++k) vt += red[1][k];
+    const double var = vt / M;
+    const double sd = var > 0.0 ? sqrt(var) : 1.0;
+    __syncthreads();
+    for (int i = t; i < M; i += blockDim.x) {
+        const double z = (zs[i] - mean) / sd;
+        zs[i] = z;
+        p.zq64[i] = z;
+        p.zq[i] = (float)z;
+    }
+    __syncthreads();
+    // padded shifted copies: copy m, index a -> qp[a+m], qp[b] = zq[b-W]
+    for (int e = t; e < 4 * p.lq; e += blockDim.x) {
+        const int m = e / p.lq, a = e - m * p.lq;
+        const int i = a + m - W;
+        p.qpad[e] = (i >= 0 && i < M) ? (float)zs[i] : CDTW_INF;
+    }
+    // envelope over [k-W, k+W] clipped to the query
+    for (int k = t; k < M; k += blockDim.x) {
+        double lo = zs[k], hi = zs[k];
+        const int a0 = max(0, k - W), a1 = min(M - 1, k + W);
+        for (int i = a0; i <= a1; ++i) {
+            lo = fmin(lo, zs[i]);
+            hi = fmax(hi, zs[i]);
+        }
+        p.env[k] = make_float2((float)lo, (float)hi);
+    }
+}
+
+}  // namespace
+
+int launch_avg_std(cdtw_handle h, const float* x, int64_t N, int M, double* mu, float* sigma) {
+    const int64_t Nw = N - M + 1;
+    const int64_t warps = div_up(Nw, kStatsWarpWindows);
+    const int64_t blocks = div_up(warps, kStatsBlock / 32);
+    avg_std_kernel<<<(unsigned)blocks, kStatsBlock, 0, h->stream>>>(x, N, M, mu, sigma);
+    CDTW_LAUNCH(h, "avg_std_kernel");
+    return CDTW_OK;
+}
+
+int launch_prepare_query(cdtw_handle h, const float* d_query_raw, int M, int W) {
+    const size_t smem = (size_t)M * sizeof(double);
+    if (smem > 48 * 1024)
+        CDTW_CUDA(h, cudaFuncSetAttribute((const void*)prepare_query_kernel,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)smem));
+    prepare_query_kernel<<<1, 256, smem, h->stream>>>(d_query_raw, M, W, h->q);
+    CDTW_LAUNCH(h, "prepare_query_kernel");
+    return CDTW_OK;
+}
+
+}  // namespace cdtw

@@ -1,0 +1,112 @@
+/*
+ * cudadtw.h -- C ABI of the B200-native z-normalised subsequence search under a
+ * Sakoe-Chiba band (the hot path of CUDA-DTW, gravitino/cudadtw).
+ *
+ * Every entry point returns an int status (CDTW_OK == 0) and never exits the
+ * process; cdtw_last_error() gives the message of the last failure on a
+ * handle.  Pointers named d_* are device pointers, h_* host pointers.  All
+ * work runs on the handle's stream.  Device work buffers belong to the handle
+ * (grow-only); callers own inputs and outputs.  One handle per host thread.
+ *
+ * Each declaration names the reference interface it replaces (file:line in
+ * the reference project).  The reference keeps the query in __constant__
+ * memory and the stream behind a texture reference set by the caller
+ * (GPU-dtw.cu:46, :82-84); here both are per-handle state, so calls on
+ * different handles are independent.
+ */
+#ifndef CUDADTW_H
+#define CUDADTW_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct cdtw_handle_s* cdtw_handle;
+
+enum cdtw_status {
+    CDTW_OK = 0,
+    CDTW_EINVAL = 1,       /* bad argument (sizes, band, null pointer)            */
+    CDTW_ENOMEM = 2,       /* device or pinned host allocation failed             */
+    CDTW_ECUDA = 3,        /* a CUDA runtime call or kernel launch failed         */
+    CDTW_ETIMEOUT = 4,     /* a bounded device-side wait gave up                  */
+    CDTW_EUNSUPPORTED = 5  /* valid request outside what this build implements     */
+};
+
+enum cdtw_metric {
+    CDTW_EUCLIDEAN = 0,    /* squared difference cell cost (EUCLIDEAN, GPU-dtw.cu:7) */
+    CDTW_MANHATTAN = 1     /* absolute difference cell cost (MANHATTAN, GPU-dtw.cu:8) */
+};
+
+enum cdtw_memloc { CDTW_HOST = 0, CDTW_DEVICE = 1 };
+
+/* Largest query length accepted (the reference's MAXQUERYSIZE is 4096,
+ * include/cdtw.cuh:8; 8192 for ED, include/ed.cuh:10). */
+#define CDTW_MAX_QUERY 8192
+
+/* ---- lifecycle ---------------------------------------------------------- */
+
+/* Replaces cudaSetDevice(0)/cudaDeviceReset() + the global symbols of
+ * GPU-dtw.cu:19-20.  Creates a handle bound to `device` and its own stream. */
+int cdtw_create(cdtw_handle* out, int device);
+int cdtw_destroy(cdtw_handle h);
+/* Run all further work on `cuda_stream` (a cudaStream_t; NULL = the handle's
+ * own stream).  The stream argument of the reference templates
+ * (cdtw.cuh:511, stats.cuh:116). */
+int cdtw_set_stream(cdtw_handle h, void* cuda_stream);
+const char* cdtw_last_error(cdtw_handle h);
+const char* cdtw_status_string(int status);
+
+/* W = M*(P*0.01), truncated: GPU-dtw.cu:27 / GPU-ldtw.cu:412. */
+int cdtw_band_from_percent(int M, int P);
+
+/* ---- statistics ----------------------------------------------------------- */
+
+/* Windowed mean and standard deviation of every length-M window of a float32
+ * series: avg_std<double> (include/stats.cuh:115-142).  The mean is returned
+ * in FP64, sigma in FP32; sigma = 1 where the variance is not positive
+ * (stats.cuh:49-50).  Sums are FP64 with a per-warp shift, so level-shifted
+ * series keep their variance (the reference's FP32 E[x^2]-mu^2 does not). */
+int cdtw_avg_std(cdtw_handle h, const float* d_series, int64_t N, int M,
+                 double* d_avg, float* d_std);
+
+/* ---- query ---------------------------------------------------------------- */
+
+/* z-normalise the query (FP64, population sigma; znormalize, stats.cuh:8-28)
+ * and build its band envelope (envelope, bounds.cuh:13-64) into handle state.
+ * Replaces the host z-norm + cudaMemcpyToSymbol(Czquery/Czlower/Czupper) of
+ * GPU-dtw.cu:67-68, :82-84.  `query_loc` is CDTW_HOST or CDTW_DEVICE. */
+int cdtw_set_query(cdtw_handle h, const float* query, int M, int W, int query_loc);
+
+/* ---- banded DTW ------------------------------------------------------------ */
+
+/* cDTW of the handle's query against listed windows of the subject:
+ * gpu_cdtw (include/cdtw.cuh:450-487, kernels :164-431).  d_indices == NULL
+ * means all N-M+1 windows in order (the raw, unpruned path of
+ * tests/test_dtw.cu:98-109).  d_out[t] is the squared (Euclidean) or absolute
+ * (Manhattan) cDTW of window d_indices[t] (or t).  d_avg/d_std come from
+ * cdtw_avg_std with the same M. */
+int cdtw_gpu_cdtw(cdtw_handle h, const float* d_subject, int64_t N,
+                  const double* d_avg, const float* d_std,
+                  const int32_t* d_indices, int64_t L, int metric, float* d_out);
+
+/* Whole unpruned all-windows cDTW from host buffers: H2D of query and subject,
+ * statistics, cDTW of every window, D2H of the N-M+1 results into h_out. */
+int cdtw_all_windows_host(cdtw_handle h, const float* h_query, int M,
+                          const float* h_subject, int64_t N, int W, int metric,
+                          float* h_out);
+
+/* ---- measurement ------------------------------------------------------------ */
+
+/* Issue-bound peak cell-update rate of the device (cells/s): the minimal cell
+ * update (FADD, 3-input FMNMX, FFMA) on independent register chains.  The
+ * roofline denominator of the cDTW kernels.  No reference counterpart (the
+ * reference reports raw timings only, tests/test_dtw.cu:100-109). */
+int cdtw_calibrate_cell_rate(cdtw_handle h, double* cells_per_second);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CUDADTW_H */

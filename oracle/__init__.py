@@ -1,0 +1,228 @@
+"""CPU oracle -- TEST INFRASTRUCTURE ONLY.
+
+ctypes bindings to ``liboracle.so`` (an FP64 restatement of the CUDA-DTW
+reference arithmetic, see cdtw_oracle.cpp) and runners for the reference's UCR
+Suite binaries compiled from source into ``oracle/_ref``.  Only the tests,
+``__graft_entry__.smoke()`` and bench.py's CPU-baseline / reference legs use
+this package; the cudadtw_b200 product never imports it.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import re
+import subprocess
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liboracle.so")
+REF_DIR = os.path.join(HERE, "_ref")
+
+_lib = None
+
+_f64p = ctypes.POINTER(ctypes.c_double)
+_f32p = ctypes.POINTER(ctypes.c_float)
+_i64p = ctypes.POINTER(ctypes.c_int64)
+_i64 = ctypes.c_int64
+_int = ctypes.c_int
+
+
+def build() -> None:
+    subprocess.run(["make", "-s", "-C", HERE, "all"], check=True)
+    if os.path.isdir("/root/reference") and not (
+            os.path.exists(os.path.join(REF_DIR, "UCR_DTW_BIN"))
+            and os.path.exists(os.path.join(REF_DIR, "UCR_ED_BIN"))):
+        subprocess.run(["make", "-s", "-C", HERE, "ref"], check=True)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        L = ctypes.CDLL(LIB_PATH)
+        sigs = {
+            "orc_znorm": (None, [_f64p, _int, _f64p]),
+            "orc_window_stats": (None, [_f32p, _i64, _int, _f64p, _f64p]),
+            "orc_cdtw_all": (None, [_f64p, _int, _f32p, _i64, _int, _int, _f64p]),
+            "orc_cdtw_list": (None, [_f64p, _int, _f32p, _i64, _int, _int, _i64p, _i64, _f64p]),
+            "orc_cdtw_pair": (ctypes.c_double, [_f64p, _f64p, _int, _int, _int]),
+            "orc_argmin": (None, [_f64p, _i64, _i64p, _f64p]),
+            "orc_envelope": (None, [_f64p, _int, _int, _f64p, _f64p]),
+            "orc_lb_kim": (None, [_f64p, _int, _f32p, _i64, _int, _f64p]),
+            "orc_lb_keogh": (None, [_f64p, _int, _int, _f32p, _i64, _int, _f64p]),
+            "orc_lb_keogh_rev": (None, [_f64p, _int, _int, _f32p, _i64, _int, _f64p]),
+            "orc_ldtw_all": (None, [_f64p, _int, _f32p, _i64, _int, _int, _f64p]),
+            "orc_ed_all": (None, [_f64p, _int, _f64p, _i64, _f64p]),
+            "orc_cdtw_ref_f32": (None, [_f32p, _int, _f32p, _f32p, _f32p, _i64p, _i64, _int,
+                                        _int, _f32p]),
+            "orc_max_threads": (_int, []),
+        }
+        for name, (res, args) in sigs.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def _p(a: np.ndarray, t):
+    return a.ctypes.data_as(t)
+
+
+def znorm(q) -> np.ndarray:
+    q = np.ascontiguousarray(q, dtype=np.float64)
+    out = np.empty_like(q)
+    lib().orc_znorm(_p(q, _f64p), q.size, _p(out, _f64p))
+    return out
+
+
+def window_stats(x: np.ndarray, m: int):
+    x = np.ascontiguousarray(x, dtype=np.float32)
+    nw = x.size - m + 1
+    mu = np.empty(nw, np.float64)
+    sd = np.empty(nw, np.float64)
+    lib().orc_window_stats(_p(x, _f32p), x.size, m, _p(mu, _f64p), _p(sd, _f64p))
+    return mu, sd
+
+
+def cdtw_all(query: np.ndarray, x: np.ndarray, w: int, euclid: bool = True) -> np.ndarray:
+    """Squared (or absolute) cDTW of the z-normalised query vs every window."""
+    zq = znorm(query)
+    x = np.ascontiguousarray(x, dtype=np.float32)
+    out = np.empty(x.size - zq.size + 1, np.float64)
+    lib().orc_cdtw_all(_p(zq, _f64p), zq.size, _p(x, _f32p), x.size, w, int(euclid),
+                       _p(out, _f64p))
+    return out
+
+
+def cdtw_list(query, x, w, idx, euclid=True) -> np.ndarray:
+    zq = znorm(query)
+    x = np.ascontiguousarray(x, dtype=np.float32)
+    idx = np.ascontiguousarray(idx, dtype=np.int64)
+    out = np.empty(idx.size, np.float64)
+    lib().orc_cdtw_list(_p(zq, _f64p), zq.size, _p(x, _f32p), x.size, w, int(euclid),
+                        _p(idx, _i64p), idx.size, _p(out, _f64p))
+    return out
+
+
+def cdtw_pair(a, b, w, euclid=True) -> float:
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    b = np.ascontiguousarray(b, dtype=np.float64)
+    return lib().orc_cdtw_pair(_p(a, _f64p), _p(b, _f64p), a.size, w, int(euclid))
+
+
+def argmin(v: np.ndarray):
+    v = np.ascontiguousarray(v, dtype=np.float64)
+    i = ctypes.c_int64()
+    val = ctypes.c_double()
+    lib().orc_argmin(_p(v, _f64p), v.size, ctypes.byref(i), ctypes.byref(val))
+    return i.value, val.value
+
+
+def envelope(q, w):
+    q = np.ascontiguousarray(q, dtype=np.float64)
+    lo = np.empty_like(q)
+    hi = np.empty_like(q)
+    lib().orc_envelope(_p(q, _f64p), q.size, w, _p(lo, _f64p), _p(hi, _f64p))
+    return lo, hi
+
+
+def lb_kim(query, x, euclid=True):
+    zq = znorm(query)
+    x = np.ascontiguousarray(x, dtype=np.float32)
+    out = np.empty(x.size - zq.size + 1, np.float64)
+    lib().orc_lb_kim(_p(zq, _f64p), zq.size, _p(x, _f32p), x.size, int(euclid), _p(out, _f64p))
+    return out
+
+
+def lb_keogh(query, x, w, euclid=True):
+    zq = znorm(query)
+    x = np.ascontiguousarray(x, dtype=np.float32)
+    out = np.empty(x.size - zq.size + 1, np.float64)
+    lib().orc_lb_keogh(_p(zq, _f64p), zq.size, w, _p(x, _f32p), x.size, int(euclid),
+                       _p(out, _f64p))
+    return out
+
+
+def lb_keogh_rev(query, x, w, euclid=True):
+    zq = znorm(query)
+    x = np.ascontiguousarray(x, dtype=np.float32)
+    out = np.empty(x.size - zq.size + 1, np.float64)
+    lib().orc_lb_keogh_rev(_p(zq, _f64p), zq.size, w, _p(x, _f32p), x.size, int(euclid),
+                           _p(out, _f64p))
+    return out
+
+
+def ldtw_all(query, x, w, euclid=True):
+    zq = znorm(query)
+    x = np.ascontiguousarray(x, dtype=np.float32)
+    out = np.empty(x.size - zq.size + 1, np.float64)
+    lib().orc_ldtw_all(_p(zq, _f64p), zq.size, _p(x, _f32p), x.size, w, int(euclid),
+                       _p(out, _f64p))
+    return out
+
+
+def ed_all(query, x):
+    zq = znorm(query)
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    out = np.empty(x.size - zq.size + 1, np.float64)
+    lib().orc_ed_all(_p(zq, _f64p), zq.size, _p(x, _f64p), x.size, _p(out, _f64p))
+    return out
+
+
+def cdtw_ref_f32(zq32, x, avg32, sd32, idx, w, nthreads):
+    """The reference's FP32 OpenMP all-windows cDTW (timing baseline)."""
+    zq32 = np.ascontiguousarray(zq32, dtype=np.float32)
+    x = np.ascontiguousarray(x, dtype=np.float32)
+    avg32 = np.ascontiguousarray(avg32, dtype=np.float32)
+    sd32 = np.ascontiguousarray(sd32, dtype=np.float32)
+    idx = np.ascontiguousarray(idx, dtype=np.int64)
+    out = np.empty(idx.size, np.float32)
+    lib().orc_cdtw_ref_f32(_p(zq32, _f32p), zq32.size, _p(x, _f32p), _p(avg32, _f32p),
+                           _p(sd32, _f32p), _p(idx, _i64p), idx.size, w, nthreads,
+                           _p(out, _f32p))
+    return out
+
+
+def max_threads() -> int:
+    return lib().orc_max_threads()
+
+
+_LOC = re.compile(r"Location\s*:\s*(-?\d+)")
+_DIST = re.compile(r"Distance\s*:\s*([-+0-9.eEinfa]+)")
+_TIME = re.compile(r"Total Execution Time\s*:\s*([0-9.eE+-]+)")
+
+
+def _run_ucr(binary: str, args: list[str]):
+    path = os.path.join(REF_DIR, binary)
+    if not os.path.exists(path):
+        raise FileNotFoundError(f"{path} missing: run `make -C oracle ref` where the "
+                                "reference sources are available")
+    out = subprocess.run([path] + args, check=True, capture_output=True, text=True).stdout
+    loc = int(_LOC.search(out).group(1))
+    dist = float(_DIST.search(out).group(1))
+    tm = _TIME.search(out)
+    return loc, dist, (float(tm.group(1)) if tm else None), out
+
+
+def ucr_dtw(x: np.ndarray, q: np.ndarray, r_arg: str):
+    """Run the reference UCR_DTW_BIN (argv: data query m R n; R<=1 is a band
+    fraction, R>1 an absolute band, UCR_DTW_BIN.cpp:417-425) on exact FP64
+    widenings of the float32 inputs.  Returns (location, distance, cpu_s, stdout)."""
+    with tempfile.TemporaryDirectory() as d:
+        xp, qp = os.path.join(d, "data.f64"), os.path.join(d, "query.f64")
+        x.astype(np.float64).tofile(xp)
+        q.astype(np.float64).tofile(qp)
+        return _run_ucr("UCR_DTW_BIN", [xp, qp, str(q.size), r_arg, str(x.size)])
+
+
+def ucr_ed(x: np.ndarray, q: np.ndarray):
+    """Run the reference UCR_ED_BIN (argv: data query m n, UCR_ED_BIN.cpp:115-135)."""
+    with tempfile.TemporaryDirectory() as d:
+        xp, qp = os.path.join(d, "data.f64"), os.path.join(d, "query.f64")
+        x.astype(np.float64).tofile(xp)
+        q.astype(np.float64).tofile(qp)
+        return _run_ucr("UCR_ED_BIN", [xp, qp, str(q.size), str(x.size)])

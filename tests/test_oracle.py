@@ -1,0 +1,104 @@
+"""CPU tests: the oracle pinned to the reference (UCR Suite outputs recorded in
+tests/golden by make_golden.py) and the reference's own property tests
+restated on the oracle."""
+import numpy as np
+import pytest
+
+import oracle
+from cudadtw_b200 import synth
+
+# UCR prints distances with 6 significant digits (std::cout default).
+UCR_PRINT_RTOL = 6e-6
+
+
+def test_oracle_search_matches_ucr_dtw(golden):
+    meta, load = golden
+    for c in meta["cases"]:
+        x, q = load(c["name"])
+        d = oracle.cdtw_all(q, x, c["W"])
+        loc, val = oracle.argmin(d)
+        assert loc == c["ucr_location"], c["name"]
+        assert abs(np.sqrt(val) - c["ucr_distance"]) <= UCR_PRINT_RTOL * c["ucr_distance"], c["name"]
+
+
+def test_oracle_search_matches_ucr_ed(golden):
+    meta, load = golden
+    for c in meta["ed_cases"]:
+        x, q = load(c["name"])
+        d = oracle.ed_all(q, x.astype(np.float64))
+        loc, val = oracle.argmin(d)
+        assert loc == c["ucr_location"], c["name"]
+        assert abs(np.sqrt(val) - c["ucr_distance"]) <= UCR_PRINT_RTOL * c["ucr_distance"]
+
+
+def test_lower_bounds_below_cdtw():
+    """tests/test_dtwbounds.cu:129-149: LB_Kim and LB_Keogh never exceed cDTW;
+    the reverse LB_Keogh (UCR_DTW_BIN.cpp:262-282) likewise."""
+    x = synth.ecg_like(6000, seed=5)
+    for m, w in [(128, 12), (64, 3), (96, 20)]:
+        q, _ = synth.cut_query(x, m, seed=m, noise=0.2)
+        d = oracle.cdtw_all(q, x, w)
+        for lb in (oracle.lb_kim(q, x), oracle.lb_keogh(q, x, w), oracle.lb_keogh_rev(q, x, w)):
+            assert np.all(lb <= d * (1 + 1e-12) + 1e-12)
+        for lb in (oracle.lb_kim(q, x, False), oracle.lb_keogh(q, x, w, False),
+                   oracle.lb_keogh_rev(q, x, w, False)):
+            assert np.all(lb <= oracle.cdtw_all(q, x, w, euclid=False) * (1 + 1e-12) + 1e-12)
+
+
+def test_cdtw_band_limits():
+    """W=0 is the z-normalised Euclidean distance; W >= M-1 is unconstrained."""
+    x = synth.random_walk(3000, seed=9)
+    q, _ = synth.cut_query(x, 50, seed=3, noise=0.3)
+    np.testing.assert_allclose(oracle.cdtw_all(q, x, 0), oracle.ed_all(q, x.astype(np.float64)),
+                               rtol=1e-12, atol=1e-12)
+    np.testing.assert_array_equal(oracle.cdtw_all(q, x, 49), oracle.cdtw_all(q, x, 200))
+    # widening the band never increases the distance
+    assert np.all(oracle.cdtw_all(q, x, 10) <= oracle.cdtw_all(q, x, 5) + 1e-12)
+
+
+def test_envelope_brute_force_matches_streaming_definition():
+    rng = np.random.default_rng(0)
+    q = rng.normal(size=77)
+    for w in (0, 1, 5, 40, 100):
+        lo, hi = oracle.envelope(q, w)
+        for i in range(q.size):
+            seg = q[max(0, i - w):i + w + 1]
+            assert lo[i] == seg.min() and hi[i] == seg.max()
+
+
+def test_reference_f32_cpu_cdtw_close_to_fp64():
+    """The FP32 restatement of openmp_cdtw (cdtw.cuh:91-157) used as the timed
+    CPU baseline agrees with the FP64 oracle at FP32 precision
+    (tests/test_dtw.cu:156-158 compares GPU and CPU at 1e-4 absolute)."""
+    x = synth.ecg_like(5000, seed=4)
+    q, _ = synth.cut_query(x, 128, seed=1, noise=0.05)
+    zq = oracle.znorm(q).astype(np.float32)
+    mu, sd = oracle.window_stats(x, 128)
+    idx = np.arange(x.size - 127, dtype=np.int64)
+    got = oracle.cdtw_ref_f32(zq, x, mu.astype(np.float32), sd.astype(np.float32), idx, 12, 2)
+    ref = oracle.cdtw_all(q, x, 12)
+    np.testing.assert_allclose(got, ref, rtol=2e-4, atol=1e-4)
+
+
+def test_ldtw_follows_reference_tie_rule():
+    """Greedy LDTW (ldtw.cuh:74-127) is an upper bound of cDTW (it is one
+    admissible path) and equals it for W=0."""
+    x = synth.ecg_like(4000, seed=6)
+    q, _ = synth.cut_query(x, 64, seed=2, noise=0.1)
+    ld = oracle.ldtw_all(q, x, 6)
+    assert np.all(ld + 1e-9 >= oracle.cdtw_all(q, x, 6))
+    np.testing.assert_allclose(oracle.ldtw_all(q, x, 0), oracle.cdtw_all(q, x, 0), rtol=1e-12)
+
+
+def test_band_formula():
+    assert synth.band_from_percent(128, 10) == 12
+    assert synth.band_from_percent(1024, 20) == 204
+    assert synth.band_from_percent(100, 7) == 7
+
+
+def test_synthetic_generators_deterministic():
+    a = synth.ecg_like(10000, seed=0)
+    b = synth.ecg_like(10000, seed=0)
+    assert a.dtype == np.float32 and np.array_equal(a, b)
+    m = synth.metal_like(300000, seed=1)
+    assert np.abs(m).max() > 100  # level-shifted regime
