@@ -23,11 +23,12 @@ HOST, DEVICE = 0, 1
 
 
 def _metric(m) -> int:
-    if m in (EUCLIDEAN, "euclidean", True):
-        return EUCLIDEAN
-    if m in (MANHATTAN, "manhattan", False):
-        return MANHATTAN
-    raise ValueError(f"unknown metric {m!r}")
+    """0 / "euclidean" -> squared cost, 1 / "manhattan" -> absolute cost."""
+    if isinstance(m, str):
+        m = {"euclidean": EUCLIDEAN, "manhattan": MANHATTAN}.get(m.lower(), -1)
+    if isinstance(m, bool) or m not in (EUCLIDEAN, MANHATTAN):
+        raise ValueError(f"unknown metric {m!r}")
+    return int(m)
 
 
 def band_from_percent(m: int, p: int) -> int:

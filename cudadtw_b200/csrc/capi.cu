@@ -131,7 +131,7 @@ int cdtw_destroy(cdtw_handle h) {
 
 int cdtw_set_stream(cdtw_handle h, void* cuda_stream) {
     if (!h) return CDTW_EINVAL;
-    h->stream = cuda_stream ? (cudaStream_t)cuda_stream : h->own_stream;
+    h->stream = (cudaStream_t)cuda_stream;  // NULL is the legacy default stream
     return CDTW_OK;
 }
 

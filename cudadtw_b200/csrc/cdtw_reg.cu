@@ -29,13 +29,17 @@ template <int W, bool EU>
 __global__ void __launch_bounds__(kRegBlock)
 cdtw_reg_kernel(const float* __restrict__ x, const double* __restrict__ mu,
                 const float* __restrict__ sigma, const float4* __restrict__ qpad4, int lq4,
-                int M, const int32_t* __restrict__ idx, int L, float* __restrict__ out) {
+                int M, int Nw, const int32_t* __restrict__ idx, int L, float* __restrict__ out) {
     extern __shared__ float4 sq4[];
     for (int e = threadIdx.x; e < 4 * lq4; e += blockDim.x) sq4[e] = qpad4[e];
     __syncthreads();
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= L) return;
     const int w = idx ? idx[t] : t;
+    if (w < 0 || w >= Nw) {  // a listed window outside the subject: NaN, no access
+        out[t] = __int_as_float(0x7fc00000);
+        return;
+    }
     const Norm nm = make_norm(mu[w], sigma[w]);
     const float* __restrict__ xw = x + w;
 
@@ -79,7 +83,7 @@ cdtw_reg_kernel(const float* __restrict__ x, const double* __restrict__ mu,
 }
 
 using RegKernel = void (*)(const float*, const double*, const float*, const float4*, int, int,
-                           const int32_t*, int, float*);
+                           int, const int32_t*, int, float*);
 
 template <int W>
 struct RegTable {
@@ -112,8 +116,8 @@ int max_register_band() { return kMaxRegW; }
 int launch_cdtw_windows(cdtw_handle h, const float* x, int64_t N, const double* mu,
                         const float* sigma, const int32_t* idx, int64_t L, bool euclid,
                         float* out) {
-    (void)N;
     const QueryPack& q = h->q;
+    const int Nw = (int)(N - q.M + 1);
     if (q.W > kMaxRegW)
         return set_error(h, CDTW_EUNSUPPORTED, "band W=%d above the register-band limit %d", q.W,
                          kMaxRegW);
@@ -126,8 +130,8 @@ int launch_cdtw_windows(cdtw_handle h, const float* x, int64_t N, const double* 
                                           cudaFuncAttributeMaxDynamicSharedMemorySize,
                                           (int)smem));
     const unsigned blocks = (unsigned)div_up(L, kRegBlock);
-    k<<<blocks, kRegBlock, smem, h->stream>>>(x, mu, sigma, (const float4*)q.qpad, lq4, q.M, idx,
-                                              (int)L, out);
+    k<<<blocks, kRegBlock, smem, h->stream>>>(x, mu, sigma, (const float4*)q.qpad, lq4, q.M, Nw,
+                                              idx, (int)L, out);
     CDTW_LAUNCH(h, "cdtw_reg_kernel");
     return CDTW_OK;
 }

@@ -51,9 +51,10 @@ enum cdtw_memloc { CDTW_HOST = 0, CDTW_DEVICE = 1 };
  * GPU-dtw.cu:19-20.  Creates a handle bound to `device` and its own stream. */
 int cdtw_create(cdtw_handle* out, int device);
 int cdtw_destroy(cdtw_handle h);
-/* Run all further work on `cuda_stream` (a cudaStream_t; NULL = the handle's
- * own stream).  The stream argument of the reference templates
- * (cdtw.cuh:511, stats.cuh:116). */
+/* Run all further work on `cuda_stream` (a cudaStream_t; NULL is the legacy
+ * default stream, as in CUDA).  Until this is called the handle uses a
+ * non-blocking stream of its own.  The stream argument of the reference
+ * templates (cdtw.cuh:511, stats.cuh:116). */
 int cdtw_set_stream(cdtw_handle h, void* cuda_stream);
 const char* cdtw_last_error(cdtw_handle h);
 const char* cdtw_status_string(int status);
