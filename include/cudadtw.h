@@ -98,6 +98,42 @@ int cdtw_all_windows_host(cdtw_handle h, const float* h_query, int M,
                           const float* h_subject, int64_t N, int W, int metric,
                           float* h_out);
 
+/* ---- fixed-scratch entry point ------------------------------------------------ */
+
+/* Limits of cdtw_all_windows_noalloc and the size of its fixed device array. */
+#define CDTW_NOALLOC_MAX_QUERY 4096
+#define CDTW_NOALLOC_MAX_WINDOWS 1048576
+#define CDTW_NOALLOC_SCRATCH_BYTES 12861696
+
+/* All-windows cDTW that allocates nothing.  No counterpart in the reference.
+ *
+ * For callers that cannot let the library allocate device memory: hosts that
+ * keep the device memory budget to themselves and lend the library only the
+ * buffers of one call, or pipelines that cannot absorb the device-wide
+ * synchronisation of cudaMalloc/cudaFree.  The handle API allocates (pinned
+ * memory and a stream at cdtw_create, device work memory on first use); this
+ * call takes no handle and calls no allocating routine.
+ *
+ * Computes the same as cdtw_set_query + cdtw_avg_std + cdtw_gpu_cdtw over all
+ * N-M+1 windows: d_out[w] = squared (CDTW_EUCLIDEAN) or absolute
+ * (CDTW_MANHATTAN) cDTW of the z-normalised raw query d_query (M floats, on
+ * the device) against window w of d_subject.  Runs on `cuda_stream` (a
+ * cudaStream_t; NULL = legacy default stream) on the current device.
+ *
+ * Working memory is one fixed __device__ array of CDTW_NOALLOC_SCRATCH_BYTES
+ * (about 12.3 MiB) that every GPU loading the library keeps until exit.
+ * Limits: M <= CDTW_NOALLOC_MAX_QUERY, N-M+1 <= CDTW_NOALLOC_MAX_WINDOWS,
+ * band W <= 40 (after clamping W to M-1); larger requests return
+ * CDTW_EUNSUPPORTED with the reason in errbuf (errlen bytes, may be NULL/0).
+ * The first call on a device looks up the array's address on that device;
+ * make that first call before any stream capture.  All calls on a device
+ * share the one array: calls whose work overlaps on the GPU (different
+ * streams, or host threads without ordering) race and corrupt each other's
+ * results; order them on one stream. */
+int cdtw_all_windows_noalloc(const float* d_query, int M, const float* d_subject, int64_t N,
+                             int W, int metric, float* d_out, void* cuda_stream,
+                             char* errbuf, int errlen);
+
 /* ---- measurement ------------------------------------------------------------ */
 
 /* Issue-bound peak cell-update rate of the device (cells/s): the minimal cell
