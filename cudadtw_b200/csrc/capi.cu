@@ -59,6 +59,8 @@ static int ensure_query_mem(cdtw_handle h, int M, int W) {
     const size_t o_env = c.take<float2>(M);
     const size_t o_zq = c.take<float>(M);
     const size_t o_zq64 = c.take<double>(M);
+    const int lqr = qrev_len(M, W);
+    const size_t o_qrev = c.take<float>(4 * (size_t)lqr);
     const size_t bytes = c.off;
     if (bytes > h->qmem_bytes) {
         if (h->qmem) {
@@ -78,6 +80,9 @@ static int ensure_query_mem(cdtw_handle h, int M, int W) {
     q.env = (float2*)(base + o_env);
     q.zq = (float*)(base + o_zq);
     q.zq64 = (double*)(base + o_zq64);
+    q.lqr = lqr;
+    q.qrev_base = qrev_hi(M, W);
+    q.qrev = (float*)(base + o_qrev);
     return CDTW_OK;
 }
 

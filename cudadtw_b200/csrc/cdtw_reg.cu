@@ -118,9 +118,13 @@ int launch_cdtw_windows(cdtw_handle h, const float* x, int64_t N, const double* 
                         float* out) {
     const QueryPack& q = h->q;
     const int Nw = (int)(N - q.M + 1);
-    if (q.W > kMaxRegW)
-        return set_error(h, CDTW_EUNSUPPORTED, "band W=%d above the register-band limit %d", q.W,
-                         kMaxRegW);
+    if (q.W > kMaxRegW) {
+        if (!q.qrev)
+            return set_error(h, CDTW_EUNSUPPORTED, "band W=%d above the register-band limit %d",
+                             q.W, kMaxRegW);
+        return launch_cdtw_strip(h, x, N, mu, sigma, idx, L, euclid, strip_rows_default(q.W),
+                                 out);
+    }
     if (L <= 0) return CDTW_OK;
     RegKernel k = euclid ? reg_kernels().eu[q.W] : reg_kernels().mh[q.W];
     const int lq4 = q.lq / 4;

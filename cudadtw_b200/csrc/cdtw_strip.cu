@@ -1,0 +1,232 @@
+// Banded DTW for wide bands ("strip" kernel): one thread per window, the
+// window processed in strips of R data rows.
+//
+// Reference: the block kernels of include/cdtw.cuh:164-363 refuse bands whose
+// W+2 lanes or 3(W+2)+M shared words do not fit (cdtw.cuh:459-465).  Here a
+// thread keeps R rows of the band in registers and walks them along
+// anti-diagonals: at step t, row r of the strip updates query column
+// c_t - r, so the R cells of a step are independent (no left-to-right chain)
+// and each depends only on the previous two steps.  The rows a strip
+// produces for the next strip (its last row, one value per query column) go
+// through a per-lane ring of 2W+2 floats in shared memory; the z-normalised
+// samples of a strip's rows stay in registers for the whole strip, and the
+// query values of a step (the same for all 32 lanes) are one broadcast
+// 16-byte load per 4 rows from four shifted copies of the reversed query.
+//
+// Band edges: row r of a strip is inside the band for steps [2r, 2W+2r]; the
+// entry and exit triangles of a strip are unrolled at compile time, so there
+// is no per-cell masking.  Matrix edges: query columns < 0 are +inf; data
+// rows and query columns >= M are extended to the next multiple of R with
+// "diagonal-only" cells: e_k = k * 1e18 at position k, so cost(k,k) = 0 and
+// every other extended cell costs >= 1e36 (or +inf).  D[M'-1][M'-1] of the
+// extended matrix therefore equals D[M-1][M-1] exactly, and it is the last
+// row of the last strip, read back from the ring.
+#include "common.cuh"
+
+namespace cdtw {
+
+namespace {
+
+constexpr int kStripWarps = 2;  // warps per block
+
+struct StripArgs {
+    const float* x;
+    const double* mu;
+    const float* sigma;
+    const float4* qrev4;  // 4 copies of the reversed extended query, lqr floats each
+    int lqr4;             // float4 per copy
+    int qbase;            // A: qrev[a] = qext[A - a]
+    int M, W, P, Nw;
+    const int32_t* idx;
+    int L;
+    float* out;
+};
+
+__device__ __forceinline__ float ext_value(int k) { return (float)k * 1e18f; }
+
+// One anti-diagonal step over rows [LO, HI] of the strip.
+//   z[r]    : z-normalised sample of row r (static for the strip)
+//   d1[r]   : row r at step t-1 (becomes row r at step t)
+//   d2[r]   : row r at step t-2 (becomes row r at step t-1)
+//   qv[r]   : query value at column c_t - r
+//   up0/dg0 : previous-strip values at columns c_t and c_t - 1 (row 0 only)
+template <int R, int LO, int HI, int KILL, bool EU>
+__device__ __forceinline__ void strip_step(const float (&z)[R], float (&d1)[R], float (&d2)[R],
+                                           const float (&qv)[R], float up0, float dg0) {
+#pragma unroll
+    for (int r = HI; r >= LO; --r) {  // bottom-up: row r-1 still holds step t-1 / t-2
+        const float up = (r == 0) ? up0 : d1[r - 1];
+        const float dg = (r == 0) ? dg0 : d2[r - 1];
+        const float v = cell<EU>(z[r] - qv[r], min3f(dg, up, d1[r]));
+        d2[r] = d1[r];
+        d1[r] = v;
+    }
+    if (KILL >= 0) {  // row KILL just left the band: it must read as +inf below
+        d2[KILL] = d1[KILL];
+        d1[KILL] = CDTW_INF;
+    }
+}
+
+template <int R>
+__device__ __forceinline__ void load_q(const StripArgs& a, int c, float (&qv)[R]) {
+    const int a0 = a.qbase - c;  // qrev index of row 0's query value
+    const float4* p = a.qrev4 + (a0 & 3) * a.lqr4 + (a0 >> 2);
+#pragma unroll
+    for (int k = 0; k < R / 4; ++k) {
+        const float4 v = __ldg(p + k);
+        qv[4 * k + 0] = v.x;
+        qv[4 * k + 1] = v.y;
+        qv[4 * k + 2] = v.z;
+        qv[4 * k + 3] = v.w;
+    }
+}
+
+// Compile-time loop over the entry triangle: steps t = T0 .. 2R-3.
+template <int R, int T, bool EU>
+struct Entry {
+    __device__ __forceinline__ static void run(const StripArgs& a, int c0, const float (&z)[R],
+                                               float (&d1)[R], float (&d2)[R], float* ring,
+                                               int& rs, float& dg0) {
+        if constexpr (T <= 2 * R - 3) {
+            float qv[R];
+            load_q<R>(a, c0 + T, qv);
+            const float up0 = ring[rs * 32];
+            strip_step<R, 0, T / 2, -1, EU>(z, d1, d2, qv, up0, dg0);
+            dg0 = up0;
+            rs = (rs + 1 == a.P) ? 0 : rs + 1;
+            Entry<R, T + 1, EU>::run(a, c0, z, d1, d2, ring, rs, dg0);
+        }
+    }
+};
+
+// Compile-time loop over the exit triangle: steps t = 2W+1+TP, TP = 0 .. 2R-3.
+template <int R, int TP, bool EU>
+struct Exit {
+    __device__ __forceinline__ static void run(const StripArgs& a, int cx, const float (&z)[R],
+                                               float (&d1)[R], float (&d2)[R], float* ring,
+                                               int& ws) {
+        if constexpr (TP <= 2 * R - 3) {
+            float qv[R];
+            load_q<R>(a, cx + TP, qv);
+            constexpr int LO = (TP + 2) / 2;  // rows r with 2r >= TP+1
+            constexpr int KILL = (TP % 2 == 0) ? TP / 2 : -1;
+            strip_step<R, LO, R - 1, KILL, EU>(z, d1, d2, qv, 0.f, 0.f);
+            ring[ws * 32] = d1[R - 1];
+            ws = (ws + 1 == a.P) ? 0 : ws + 1;
+            Exit<R, TP + 1, EU>::run(a, cx, z, d1, d2, ring, ws);
+        }
+    }
+};
+
+template <int R, bool EU>
+__global__ void __launch_bounds__(kStripWarps * 32)
+cdtw_strip_kernel(const StripArgs a) {
+    extern __shared__ float ring_all[];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    float* ring = ring_all + (size_t)wid * a.P * 32 + lane;  // slot s at ring[s * 32]
+    const int t_id = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t_id >= a.L) return;  // lanes are independent: no warp-wide operation below
+    const int w = a.idx ? a.idx[t_id] : t_id;
+    if (w < 0 || w >= a.Nw) {  // a listed window outside the subject: NaN, no access
+        a.out[t_id] = __int_as_float(0x7fc00000);
+        return;
+    }
+    const Norm nm = make_norm(a.mu[w], a.sigma[w]);
+    const float* __restrict__ xw = a.x + w;
+    const int M = a.M, W = a.W, P = a.P;
+    // ring holds previous-strip row values by query column, slot = col mod P;
+    // virtual row -1: D[-1][-1] = 0, +inf elsewhere
+    for (int s = 0; s < P; ++s) ring[s * 32] = CDTW_INF;
+    ring[(P - 1) * 32] = 0.0f;  // column -1
+    const int S = (M + R - 1) / R;
+    const int n_int = 2 * W - 2 * R + 3;  // interior steps t = 2R-2 .. 2W (W >= R-1)
+    for (int s = 0; s < S; ++s) {
+        const int j0 = s * R;
+        float z[R], d1[R], d2[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            const int j = j0 + r;
+            z[r] = (j < M) ? znorm(nm, __ldg(xw + j)) : ext_value(j);
+            d1[r] = CDTW_INF;
+            d2[r] = CDTW_INF;
+        }
+        const int c0 = j0 - W;  // row 0's column at step 0
+        int rs = ((c0 % P) + P) % P;                      // read slot: column c_t
+        int ws = (((c0 - (R - 1)) % P) + P) % P;          // write slot: column c_t - (R-1)
+        float dg0 = ring[(rs == 0 ? P - 1 : rs - 1) * 32];  // column c0 - 1
+        // entry triangle: t = 0 .. 2R-3 (no writes yet: row R-1 starts at 2R-2)
+        Entry<R, 0, EU>::run(a, c0, z, d1, d2, ring, rs, dg0);
+        // ws must track the column c_t - (R-1) for the first write at t = 2R-2
+        ws = (ws + 2 * R - 2) % P;
+        // interior: all rows active, read row 0's boundary, write row R-1's
+        int c = c0 + 2 * R - 2;
+#pragma unroll 2
+        for (int it = 0; it < n_int; ++it, ++c) {
+            float qv[R];
+            load_q<R>(a, c, qv);
+            const float up0 = ring[rs * 32];
+            strip_step<R, 0, R - 1, -1, EU>(z, d1, d2, qv, up0, dg0);
+            dg0 = up0;
+            rs = (rs + 1 == P) ? 0 : rs + 1;
+            ring[ws * 32] = d1[R - 1];
+            ws = (ws + 1 == P) ? 0 : ws + 1;
+        }
+        // exit triangle: t = 2W+1 .. 2W+2R-2 (row 0 done, no reads)
+        Exit<R, 0, EU>::run(a, c0 + 2 * W + 1, z, d1, d2, ring, ws);
+        ring[ws * 32] = CDTW_INF;  // column j0+R+W: outside the next strip's upper band edge
+    }
+    // D[M'-1][M'-1] of the extended matrix = D[M-1][M-1]; it sits at column M'-1
+    const int colf = S * R - 1;
+    a.out[t_id] = ring[(colf % P) * 32];
+}
+
+using StripKernel = void (*)(const StripArgs);
+
+}  // namespace
+
+int strip_rows_default(int W) { return W >= 63 ? 32 : 16; }
+
+// Strip kernel launch for bands W >= R-1.  R in {16, 32}.
+int launch_cdtw_strip(cdtw_handle h, const float* x, int64_t N, const double* mu,
+                      const float* sigma, const int32_t* idx, int64_t L, bool euclid, int R,
+                      float* out) {
+    const QueryPack& q = h->q;
+    if (R != 16 && R != 32) return set_error(h, CDTW_EINVAL, "strip rows must be 16 or 32");
+    if (q.W < R - 1)
+        return set_error(h, CDTW_EUNSUPPORTED, "strip kernel needs W >= R-1 (W=%d R=%d)", q.W, R);
+    if (L <= 0) return CDTW_OK;
+    StripArgs a;
+    a.x = x;
+    a.mu = mu;
+    a.sigma = sigma;
+    a.qrev4 = (const float4*)q.qrev;
+    a.lqr4 = q.lqr / 4;
+    a.qbase = q.qrev_base;
+    a.M = q.M;
+    a.W = q.W;
+    a.P = 2 * q.W + 2;
+    a.Nw = (int)(N - q.M + 1);
+    a.idx = idx;
+    a.L = (int)L;
+    a.out = out;
+    StripKernel k;
+    if (R == 16) k = euclid ? cdtw_strip_kernel<16, true> : cdtw_strip_kernel<16, false>;
+    else k = euclid ? cdtw_strip_kernel<32, true> : cdtw_strip_kernel<32, false>;
+    // two warps per block when their rings fit, else one
+    const size_t ring_warp = (size_t)a.P * 32 * sizeof(float);
+    const int warps = (2 * ring_warp <= 227 * 1024) ? 2 : 1;
+    const size_t smem = warps * ring_warp;
+    if (smem > 227 * 1024)
+        return set_error(h, CDTW_EUNSUPPORTED, "band W=%d needs %zu B of shared memory", q.W,
+                         smem);
+    if (smem > 48 * 1024)
+        CDTW_CUDA(h, cudaFuncSetAttribute((const void*)k,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)smem));
+    const unsigned blocks = (unsigned)div_up(L, warps * 32);
+    k<<<blocks, warps * 32, smem, h->stream>>>(a);
+    CDTW_LAUNCH(h, "cdtw_strip_kernel");
+    return CDTW_OK;
+}
+
+}  // namespace cdtw

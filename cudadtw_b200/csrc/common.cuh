@@ -25,6 +25,10 @@ namespace cdtw {
 //           copy (j&3) at index (j&~3).
 //   env   : (L_k, U_k) pairs of the query envelope over +-W.
 //   zq    : z-normalised query (float).
+//   qrev  : 4 shifted copies of the reversed, extended query read by the strip
+//           kernel: copy m holds qr[a+m], qr[b] = qext[qrev_base - b], with
+//           qext[i] = +inf (i < 0), zq[i] (0 <= i < M), i*1e18 (i >= M).
+//           Optional (nullptr: not built).
 struct QueryPack {
     int M = 0, W = 0;
     int lq = 0;            // floats per qpad copy (multiple of 4)
@@ -32,7 +36,18 @@ struct QueryPack {
     float2* env = nullptr; // M pairs
     float* zq = nullptr;   // M floats
     double* zq64 = nullptr;// M doubles
+    int lqr = 0;           // floats per qrev copy (multiple of 4)
+    int qrev_base = 0;     // A
+    float* qrev = nullptr; // 4 * lqr floats
 };
+
+// Extent of the reversed extended query for strips of up to kStripRowsMax rows.
+constexpr int kStripRowsMax = 32;
+__host__ __device__ inline int qrev_lo(int W) { return -(W + kStripRowsMax + 8); }
+__host__ __device__ inline int qrev_hi(int M, int W) { return M + W + 3 * kStripRowsMax + 8; }
+__host__ __device__ inline int qrev_len(int M, int W) {
+    return (qrev_hi(M, W) - qrev_lo(W) + 1 + 4 + 3) / 4 * 4;
+}
 
 }  // namespace cdtw
 
@@ -130,5 +145,10 @@ int launch_prepare_query(cdtw_handle h, const float* d_query_raw, int M, int W);
 int launch_cdtw_windows(cdtw_handle h, const float* x, int64_t N, const double* mu,
                         const float* sigma, const int32_t* idx, int64_t L, bool euclid,
                         float* out);
+int launch_cdtw_strip(cdtw_handle h, const float* x, int64_t N, const double* mu,
+                      const float* sigma, const int32_t* idx, int64_t L, bool euclid, int R,
+                      float* out);
+int strip_rows_default(int W);
+int max_register_band();
 
 }  // namespace cdtw

@@ -123,6 +123,19 @@ prepare_query_kernel(const float* __restrict__ qraw, int M, int W, QueryPack p) 
         const int i = a + m - W;
         p.qpad[e] = (i >= 0 && i < M) ? (float)zs[i] : CDTW_INF;
     }
+    // reversed extended copies for the strip kernel
+    if (p.qrev) {
+        const int lo = qrev_lo(W), A = p.qrev_base, len = qrev_hi(M, W) - lo + 1;
+        for (int e = t; e < 4 * p.lqr; e += blockDim.x) {
+            const int m = e / p.lqr, b = e - m * p.lqr + m;  // qr index
+            float v = CDTW_INF;
+            if (b < len) {
+                const int i = A - b;
+                v = (i < 0) ? CDTW_INF : (i < M ? (float)zs[i] : (float)i * 1e18f);
+            }
+            p.qrev[e] = v;
+        }
+    }
     // envelope over [k-W, k+W] clipped to the query
     for (int k = t; k < M; k += blockDim.x) {
         double lo = zs[k], hi = zs[k];

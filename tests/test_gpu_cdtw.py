@@ -126,3 +126,31 @@ def test_errors_are_status_codes(handle):
     assert e.value.status == 1
     with pytest.raises(CudaDTWError):
         handle.set_query(np.zeros(0, np.float32), 3)
+
+
+@pytest.mark.parametrize("m,w,nwin", [(128, 41, 3000), (256, 51, 3000), (300, 62, 2000),
+                                      (300, 63, 2000), (512, 102, 1500), (1024, 204, 600),
+                                      (2048, 409, 200), (777, 300, 300)])
+def test_all_windows_wide_bands(handle, m, w, nwin):
+    """Bands above the register-band limit run on the strip kernel."""
+    x = synth.metal_like(m + nwin - 1, seed=w)
+    q, _ = synth.cut_query(x, m, seed=w, noise=0.2)
+    got = _all_windows(handle, q, x, w)
+    np.testing.assert_allclose(got, oracle.cdtw_all(q, x, w), rtol=RTOL, atol=ATOL)
+    got1 = _all_windows(handle, q, x, w, metric=1)
+    np.testing.assert_allclose(got1, oracle.cdtw_all(q, x, w, euclid=False), rtol=RTOL, atol=ATOL)
+
+
+def test_strip_kernel_index_list(handle):
+    x = synth.ecg_like(20000, seed=5)
+    q, _ = synth.cut_query(x, 512, seed=5, noise=0.05)
+    dx = _dev(x)
+    avg, std = handle.avg_std(dx, 512)
+    handle.set_query(q, 102)
+    idx = np.random.default_rng(1).permutation(x.size - 511)[:500].astype(np.int32)
+    idx[7] = x.size  # outside the subject: NaN, no access
+    got = handle.gpu_cdtw(dx, avg, std, indices=_dev(idx)).cpu().numpy()
+    full = handle.gpu_cdtw(dx, avg, std).cpu().numpy()
+    assert np.isnan(got[7])
+    keep = np.arange(idx.size) != 7
+    np.testing.assert_array_equal(got[keep], full[idx[keep]])
