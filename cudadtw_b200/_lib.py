@@ -29,6 +29,11 @@ SIGNATURES = {
     "cdtw_gpu_cdtw": (c_int, [c_vp, c_vp, c_i64, c_vp, c_vp, c_vp, c_i64, c_int, c_vp]),
     "cdtw_all_windows_host": (c_int, [c_vp, c_vp, c_int, c_vp, c_i64, c_int, c_int, c_vp]),
     "cdtw_calibrate_cell_rate": (c_int, [c_vp, c_f64p]),
+    "cdtw_lb_kim": (c_int, [c_vp, c_vp, c_i64, c_vp, c_vp, c_vp, c_i64, c_int, c_vp]),
+    "cdtw_lb_keogh": (c_int, [c_vp, c_vp, c_i64, c_vp, c_vp, c_vp, c_i64, c_int, c_vp, c_vp]),
+    "cdtw_prune_cdtw": (c_int, [c_vp, c_vp, c_i64, c_vp, c_vp, c_int, c_i64p, c_f32p]),
+    "cdtw_search_host": (c_int, [c_vp, c_vp, c_int, c_vp, c_i64, c_int, c_int, c_i64p, c_f32p]),
+    "cdtw_search_counts": (c_int, [c_vp, c_i64p]),
     "cdtw_all_windows_noalloc": (c_int, [c_vp, c_int, c_vp, c_i64, c_int, c_int, c_vp, c_vp,
                                          ctypes.c_char_p, c_int]),
 }

@@ -154,3 +154,53 @@ class Handle:
         self._check(self._lib.cdtw_all_windows_host(self._h, _ptr(q), q.size, _ptr(s), s.size, W,
                                                     _metric(metric), _ptr(out)))
         return out
+
+    # -- lower bounds and search ---------------------------------------------
+    def lb_kim(self, subject, avg, std, indices=None, metric=EUCLIDEAN):
+        """LB_Kim (5x5 front/back, include/bounds.cuh:413-441) per window."""
+        n = indices.numel() if indices is not None else subject.numel() - self.M + 1
+        out = torch.empty(n, dtype=torch.float32, device=subject.device)
+        self._check(self._lib.cdtw_lb_kim(self._h, _ptr(subject), subject.numel(), _ptr(avg),
+                                          _ptr(std), _ptr(indices), n, _metric(metric),
+                                          _ptr(out)))
+        return out
+
+    def lb_keogh(self, subject, avg, std, indices=None, metric=EUCLIDEAN, reverse=True):
+        """(forward LB_Keogh, reverse LB_Keogh) per window (bounds.cuh:443-465;
+        UCR_DTW_BIN.cpp:262-282)."""
+        n = indices.numel() if indices is not None else subject.numel() - self.M + 1
+        fwd = torch.empty(n, dtype=torch.float32, device=subject.device)
+        rev = torch.empty(n, dtype=torch.float32, device=subject.device) if reverse else None
+        self._check(self._lib.cdtw_lb_keogh(self._h, _ptr(subject), subject.numel(), _ptr(avg),
+                                            _ptr(std), _ptr(indices), n, _metric(metric),
+                                            _ptr(fwd), _ptr(rev)))
+        return fwd, rev
+
+    def prune_cdtw(self, subject, avg, std, metric=EUCLIDEAN):
+        """Best match (location, distance) of the query (prune_cdtw,
+        include/cdtw.cuh:510-592); distance as the reference prints it."""
+        loc = ctypes.c_int64()
+        dist = ctypes.c_float()
+        self._check(self._lib.cdtw_prune_cdtw(self._h, _ptr(subject), subject.numel(), _ptr(avg),
+                                              _ptr(std), _metric(metric), ctypes.byref(loc),
+                                              ctypes.byref(dist)))
+        return loc.value, dist.value
+
+    def search_host(self, query, subject, W, metric=EUCLIDEAN):
+        """The whole GPU-DTW search from host arrays (GPU-dtw.cu:59-90)."""
+        q = np.ascontiguousarray(query, dtype=np.float32)
+        s = subject if (isinstance(subject, np.ndarray) and subject.dtype == np.float32
+                        and subject.flags.c_contiguous) else np.ascontiguousarray(subject, np.float32)
+        loc = ctypes.c_int64()
+        dist = ctypes.c_float()
+        self._check(self._lib.cdtw_search_host(self._h, _ptr(q), q.size, _ptr(s), s.size, W,
+                                               _metric(metric), ctypes.byref(loc),
+                                               ctypes.byref(dist)))
+        self.M, self.W = q.size, min(W, q.size - 1)
+        return loc.value, dist.value
+
+    def search_counts(self):
+        """(windows, below bsf after LB_Kim, reaching cDTW) of the last search."""
+        c = (ctypes.c_int64 * 3)()
+        self._check(self._lib.cdtw_search_counts(self._h, c))
+        return tuple(c)

@@ -88,6 +88,31 @@ static int ensure_query_mem(cdtw_handle h, int M, int W) {
 
 static bool valid_metric(int metric) { return metric == CDTW_EUCLIDEAN || metric == CDTW_MANHATTAN; }
 
+// Reads the search result key and stage counts back (the one host sync).
+static int finish_search(cdtw_handle h, const unsigned long long* key, const int* ctr, int64_t Nw,
+                         bool euclid, int64_t* location, float* distance) {
+    char* pin = (char*)h->pinned;
+    CDTW_CUDA(h, cudaMemcpyAsync(pin, key, sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                                 h->stream));
+    CDTW_CUDA(h, cudaMemcpyAsync(pin + 8, ctr, sizeof(int) * 2, cudaMemcpyDeviceToHost,
+                                 h->stream));
+    CDTW_CUDA(h, cudaStreamSynchronize(h->stream));
+    unsigned long long k;
+    int c[2];
+    memcpy(&k, pin, 8);
+    memcpy(c, pin + 8, 8);
+    h->last_counts[0] = Nw;
+    h->last_counts[1] = c[0];
+    h->last_counts[2] = c[1];
+    if (k == ~0ull) return set_error(h, CDTW_ECUDA, "search produced no result");
+    const uint32_t bits = (uint32_t)(k >> 32);
+    float d;
+    memcpy(&d, &bits, 4);
+    if (location) *location = (int64_t)(uint32_t)k;
+    if (distance) *distance = euclid ? sqrtf(d) : d;
+    return CDTW_OK;
+}
+
 }  // namespace cdtw
 
 using namespace cdtw;
@@ -237,6 +262,104 @@ int cdtw_all_windows_host(cdtw_handle h, const float* h_query, int M, const floa
     CDTW_CUDA(h, cudaMemcpyAsync(h_out, dout, sizeof(float) * Nw, cudaMemcpyDeviceToHost,
                                  h->stream));
     CDTW_CUDA(h, cudaStreamSynchronize(h->stream));
+    return CDTW_OK;
+}
+
+int cdtw_lb_kim(cdtw_handle h, const float* d_subject, int64_t N, const double* d_avg,
+                const float* d_std, const int32_t* d_indices, int64_t L, int metric,
+                float* d_out) {
+    if (!h) return CDTW_EINVAL;
+    if (!h->has_query) return set_error(h, CDTW_EINVAL, "no query set (cdtw_set_query)");
+    if (!d_subject || !d_avg || !d_std || !d_out) return set_error(h, CDTW_EINVAL, "null pointer");
+    if (!valid_metric(metric)) return set_error(h, CDTW_EINVAL, "bad metric %d", metric);
+    if (N < h->q.M) return set_error(h, CDTW_EINVAL, "subject shorter than query");
+    if (!d_indices) L = N - h->q.M + 1;
+    if (L < 0 || L > INT32_MAX) return set_error(h, CDTW_EINVAL, "bad index count");
+    CDTW_CUDA(h, cudaSetDevice(h->device));
+    return launch_lb_kim(h, d_subject, N, d_avg, d_std, d_indices, L, metric == CDTW_EUCLIDEAN,
+                         d_out, nullptr);
+}
+
+int cdtw_lb_keogh(cdtw_handle h, const float* d_subject, int64_t N, const double* d_avg,
+                  const float* d_std, const int32_t* d_indices, int64_t L, int metric,
+                  float* d_fwd, float* d_rev) {
+    if (!h) return CDTW_EINVAL;
+    if (!h->has_query) return set_error(h, CDTW_EINVAL, "no query set (cdtw_set_query)");
+    if (!d_subject || !d_avg || !d_std || (!d_fwd && !d_rev))
+        return set_error(h, CDTW_EINVAL, "null pointer");
+    if (!valid_metric(metric)) return set_error(h, CDTW_EINVAL, "bad metric %d", metric);
+    if (N < h->q.M) return set_error(h, CDTW_EINVAL, "subject shorter than query");
+    if (!d_indices) L = N - h->q.M + 1;
+    if (L < 0 || L > INT32_MAX) return set_error(h, CDTW_EINVAL, "bad index count");
+    CDTW_CUDA(h, cudaSetDevice(h->device));
+    float2* xenv = nullptr;
+    if (d_rev) {
+        Carver c;
+        const size_t o_env = c.take<float2>(N);
+        const size_t o_scr = c.take<char>(stream_envelope_scratch_bytes(N));
+        CDTW_TRY(ensure_workspace(h, c.off));
+        xenv = (float2*)((char*)h->ws + o_env);
+        CDTW_TRY(launch_stream_envelope(h, d_subject, N, h->q.W, (float*)((char*)h->ws + o_scr),
+                                        xenv));
+    }
+    return launch_lb_keogh(h, d_subject, N, d_avg, d_std, xenv, d_indices, L,
+                           metric == CDTW_EUCLIDEAN, d_fwd, d_rev);
+}
+
+int cdtw_prune_cdtw(cdtw_handle h, const float* d_subject, int64_t N, const double* d_avg,
+                    const float* d_std, int metric, int64_t* location, float* distance) {
+    if (!h) return CDTW_EINVAL;
+    if (!h->has_query) return set_error(h, CDTW_EINVAL, "no query set (cdtw_set_query)");
+    if (!d_subject || !d_avg || !d_std) return set_error(h, CDTW_EINVAL, "null pointer");
+    if (!valid_metric(metric)) return set_error(h, CDTW_EINVAL, "bad metric %d", metric);
+    const int M = h->q.M;
+    if (M < 11)
+        return set_error(h, CDTW_EINVAL,
+                         "the search's LB_Kim is a 10-point DTW: query length must be >= 11");
+    if (N < M) return set_error(h, CDTW_EINVAL, "subject shorter than query");
+    if (N - M + 1 > INT32_MAX) return set_error(h, CDTW_EUNSUPPORTED, "too many windows");
+    CDTW_CUDA(h, cudaSetDevice(h->device));
+    CDTW_TRY(ensure_workspace(h, search_workspace_bytes(N, M)));
+    unsigned long long* key;
+    int* ctr;
+    CDTW_TRY(run_search(h, d_subject, N, d_avg, d_std, metric == CDTW_EUCLIDEAN, (char*)h->ws,
+                        &key, &ctr));
+    return finish_search(h, key, ctr, N - M + 1, metric == CDTW_EUCLIDEAN, location, distance);
+}
+
+int cdtw_search_host(cdtw_handle h, const float* h_query, int M, const float* h_subject,
+                     int64_t N, int W, int metric, int64_t* location, float* distance) {
+    if (!h) return CDTW_EINVAL;
+    if (!h_query || !h_subject) return set_error(h, CDTW_EINVAL, "null pointer");
+    if (!valid_metric(metric)) return set_error(h, CDTW_EINVAL, "bad metric %d", metric);
+    if (M < 11) return set_error(h, CDTW_EINVAL, "query length must be >= 11 (LB_Kim)");
+    if (N < M) return set_error(h, CDTW_EINVAL, "subject shorter than query");
+    const int64_t Nw = N - M + 1;
+    if (Nw > INT32_MAX) return set_error(h, CDTW_EUNSUPPORTED, "too many windows");
+    CDTW_CUDA(h, cudaSetDevice(h->device));
+    Carver c;
+    const size_t o_x = c.take<float>(N);
+    const size_t o_mu = c.take<double>(Nw);
+    const size_t o_sd = c.take<float>(Nw);
+    const size_t o_ws = c.take<char>(search_workspace_bytes(N, M));
+    CDTW_TRY(ensure_workspace(h, c.off));
+    char* base = (char*)h->ws;
+    float* dx = (float*)(base + o_x);
+    double* dmu = (double*)(base + o_mu);
+    float* dsd = (float*)(base + o_sd);
+    CDTW_CUDA(h, cudaMemcpyAsync(dx, h_subject, sizeof(float) * N, cudaMemcpyHostToDevice,
+                                 h->stream));
+    CDTW_TRY(cdtw_set_query(h, h_query, M, W, CDTW_HOST));
+    CDTW_TRY(launch_avg_std(h, dx, N, M, dmu, dsd));
+    unsigned long long* key;
+    int* ctr;
+    CDTW_TRY(run_search(h, dx, N, dmu, dsd, metric == CDTW_EUCLIDEAN, base + o_ws, &key, &ctr));
+    return finish_search(h, key, ctr, Nw, metric == CDTW_EUCLIDEAN, location, distance);
+}
+
+int cdtw_search_counts(cdtw_handle h, int64_t* counts) {
+    if (!h || !counts) return CDTW_EINVAL;
+    for (int i = 0; i < 3; ++i) counts[i] = h->last_counts[i];
     return CDTW_OK;
 }
 

@@ -23,6 +23,8 @@
 // row of the last strip, read back from the ring.
 #include "common.cuh"
 
+#include <algorithm>
+
 namespace cdtw {
 
 namespace {
@@ -104,7 +106,7 @@ template <int R, int TP, bool EU>
 struct Exit {
     __device__ __forceinline__ static void run(const StripArgs& a, int cx, const float (&z)[R],
                                                float (&d1)[R], float (&d2)[R], float* ring,
-                                               int& ws) {
+                                               int& ws, float& rmin) {
         if constexpr (TP <= 2 * R - 3) {
             float qv[R];
             load_q<R>(a, cx + TP, qv);
@@ -112,25 +114,20 @@ struct Exit {
             constexpr int KILL = (TP % 2 == 0) ? TP / 2 : -1;
             strip_step<R, LO, R - 1, KILL, EU>(z, d1, d2, qv, 0.f, 0.f);
             ring[ws * 32] = d1[R - 1];
+            rmin = fminf(rmin, d1[R - 1]);
             ws = (ws + 1 == a.P) ? 0 : ws + 1;
-            Exit<R, TP + 1, EU>::run(a, cx, z, d1, d2, ring, ws);
+            Exit<R, TP + 1, EU>::run(a, cx, z, d1, d2, ring, ws, rmin);
         }
     }
 };
 
-template <int R, bool EU>
-__global__ void __launch_bounds__(kStripWarps * 32)
-cdtw_strip_kernel(const StripArgs a) {
-    extern __shared__ float ring_all[];
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    float* ring = ring_all + (size_t)wid * a.P * 32 + lane;  // slot s at ring[s * 32]
-    const int t_id = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t_id >= a.L) return;  // lanes are independent: no warp-wide operation below
-    const int w = a.idx ? a.idx[t_id] : t_id;
-    if (w < 0 || w >= a.Nw) {  // a listed window outside the subject: NaN, no access
-        a.out[t_id] = __int_as_float(0x7fc00000);
-        return;
-    }
+// DTW of window w through the strips.  SEARCH: abandon (return +inf) once the
+// last row of a strip plus the remaining forward LB_Keogh suffix reaches the
+// best-so-far for every lane of the warp; all 32 lanes must call together.
+template <int R, bool EU, bool SEARCH>
+__device__ __forceinline__ float strip_dtw(const StripArgs& a, int w, float* ring,
+                                           const float2* __restrict__ qenv, float lbk,
+                                           bool& alive, const unsigned long long* key) {
     const Norm nm = make_norm(a.mu[w], a.sigma[w]);
     const float* __restrict__ xw = a.x + w;
     const int M = a.M, W = a.W, P = a.P;
@@ -140,6 +137,7 @@ cdtw_strip_kernel(const StripArgs a) {
     ring[(P - 1) * 32] = 0.0f;  // column -1
     const int S = (M + R - 1) / R;
     const int n_int = 2 * W - 2 * R + 3;  // interior steps t = 2R-2 .. 2W (W >= R-1)
+    float pre = 0.f;
     for (int s = 0; s < S; ++s) {
         const int j0 = s * R;
         float z[R], d1[R], d2[R];
@@ -149,6 +147,11 @@ cdtw_strip_kernel(const StripArgs a) {
             z[r] = (j < M) ? znorm(nm, __ldg(xw + j)) : ext_value(j);
             d1[r] = CDTW_INF;
             d2[r] = CDTW_INF;
+            if (SEARCH && j < M) {
+                const float2 e = __ldg(qenv + j);
+                const float dl = max3f(z[r] - e.y, e.x - z[r], 0.f);
+                pre += EU ? dl * dl : dl;
+            }
         }
         const int c0 = j0 - W;  // row 0's column at step 0
         int rs = ((c0 % P) + P) % P;                      // read slot: column c_t
@@ -158,6 +161,7 @@ cdtw_strip_kernel(const StripArgs a) {
         Entry<R, 0, EU>::run(a, c0, z, d1, d2, ring, rs, dg0);
         // ws must track the column c_t - (R-1) for the first write at t = 2R-2
         ws = (ws + 2 * R - 2) % P;
+        float rmin = CDTW_INF;  // minimum of the strip's last row (search only)
         // interior: all rows active, read row 0's boundary, write row R-1's
         int c = c0 + 2 * R - 2;
 #pragma unroll 2
@@ -169,15 +173,66 @@ cdtw_strip_kernel(const StripArgs a) {
             dg0 = up0;
             rs = (rs + 1 == P) ? 0 : rs + 1;
             ring[ws * 32] = d1[R - 1];
+            if (SEARCH) rmin = fminf(rmin, d1[R - 1]);
             ws = (ws + 1 == P) ? 0 : ws + 1;
         }
         // exit triangle: t = 2W+1 .. 2W+2R-2 (row 0 done, no reads)
-        Exit<R, 0, EU>::run(a, c0 + 2 * W + 1, z, d1, d2, ring, ws);
+        Exit<R, 0, EU>::run(a, c0 + 2 * W + 1, z, d1, d2, ring, ws, rmin);
         ring[ws * 32] = CDTW_INF;  // column j0+R+W: outside the next strip's upper band edge
+        if (SEARCH && j0 + R < M) {  // the strip's last row is a real row before M-1
+            const float bsf = load_bsf(key);
+            alive = alive && (rmin + (lbk - pre) * kLbSlack < bsf);
+            if (!__any_sync(0xffffffffu, alive)) return CDTW_INF;
+        }
     }
     // D[M'-1][M'-1] of the extended matrix = D[M-1][M-1]; it sits at column M'-1
-    const int colf = S * R - 1;
-    a.out[t_id] = ring[(colf % P) * 32];
+    return ring[(((S * R - 1) % P)) * 32];
+}
+
+template <int R, bool EU>
+__global__ void __launch_bounds__(kStripWarps * 32)
+cdtw_strip_kernel(const StripArgs a) {
+    extern __shared__ float ring_all[];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    float* ring = ring_all + (size_t)wid * a.P * 32 + lane;  // slot s at ring[s * 32]
+    const int t_id = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t_id >= a.L) return;  // lanes are independent in this mode
+    const int w = a.idx ? a.idx[t_id] : t_id;
+    if (w < 0 || w >= a.Nw) {  // a listed window outside the subject: NaN, no access
+        a.out[t_id] = __int_as_float(0x7fc00000);
+        return;
+    }
+    bool alive = true;
+    a.out[t_id] = strip_dtw<R, EU, false>(a, w, ring, nullptr, 0.f, alive, nullptr);
+}
+
+// Search variant: persistent warps over a candidate list (see the register
+// kernel's search variant for the protocol).
+template <int R, bool EU>
+__global__ void __launch_bounds__(kStripWarps * 32)
+cdtw_strip_search_kernel(const StripArgs a, const float2* __restrict__ qenv,
+                         const Cand* __restrict__ cands, const int* __restrict__ count,
+                         int* __restrict__ work, unsigned long long* __restrict__ key) {
+    extern __shared__ float ring_all[];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    float* ring = ring_all + (size_t)wid * a.P * 32 + lane;
+    const int n = *(const volatile int*)count;
+    for (;;) {
+        int base = 0;
+        if (lane == 0) base = atomicAdd(work, 32);
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (base >= n) break;
+        const int i = base + lane;
+        Cand c;
+        c.w = 0;
+        c.lb = CDTW_INF;
+        c.lbk = 0.f;
+        if (i < n) c = cands[i];
+        bool alive = (i < n) && (c.lb * kLbSlack < load_bsf(key));
+        if (!__any_sync(0xffffffffu, alive)) continue;
+        const float res = strip_dtw<R, EU, true>(a, c.w, ring, qenv, c.lbk, alive, key);
+        if (i < n && res < CDTW_INF) atomicMin(key, pack_key(res, (uint32_t)c.w));
+    }
 }
 
 using StripKernel = void (*)(const StripArgs);
@@ -226,6 +281,54 @@ int launch_cdtw_strip(cdtw_handle h, const float* x, int64_t N, const double* mu
     const unsigned blocks = (unsigned)div_up(L, warps * 32);
     k<<<blocks, warps * 32, smem, h->stream>>>(a);
     CDTW_LAUNCH(h, "cdtw_strip_kernel");
+    return CDTW_OK;
+}
+
+int launch_cdtw_strip_search(cdtw_handle h, const float* x, int64_t N, const double* mu,
+                             const float* sigma, const Cand* cands, const int* count, int* work,
+                             int max_count, bool euclid, int R, unsigned long long* key) {
+    const QueryPack& q = h->q;
+    if (R != 16 && R != 32) return set_error(h, CDTW_EINVAL, "strip rows must be 16 or 32");
+    if (q.W < R - 1)
+        return set_error(h, CDTW_EUNSUPPORTED, "strip kernel needs W >= R-1 (W=%d R=%d)", q.W, R);
+    if (max_count <= 0) return CDTW_OK;
+    StripArgs a;
+    a.x = x;
+    a.mu = mu;
+    a.sigma = sigma;
+    a.qrev4 = (const float4*)q.qrev;
+    a.lqr4 = q.lqr / 4;
+    a.qbase = q.qrev_base;
+    a.M = q.M;
+    a.W = q.W;
+    a.P = 2 * q.W + 2;
+    a.Nw = (int)(N - q.M + 1);
+    a.idx = nullptr;
+    a.L = 0;
+    a.out = nullptr;
+    using SK = void (*)(const StripArgs, const float2*, const Cand*, const int*, int*,
+                        unsigned long long*);
+    SK k;
+    if (R == 16)
+        k = euclid ? cdtw_strip_search_kernel<16, true> : cdtw_strip_search_kernel<16, false>;
+    else
+        k = euclid ? cdtw_strip_search_kernel<32, true> : cdtw_strip_search_kernel<32, false>;
+    const size_t ring_warp = (size_t)a.P * 32 * sizeof(float);
+    const int warps = (2 * ring_warp <= 227 * 1024) ? 2 : 1;
+    const size_t smem = warps * ring_warp;
+    if (smem > 227 * 1024)
+        return set_error(h, CDTW_EUNSUPPORTED, "band W=%d needs %zu B of shared memory", q.W,
+                         smem);
+    CDTW_CUDA(h, cudaFuncSetAttribute((const void*)k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)smem));
+    int per_sm = 0;
+    CDTW_CUDA(h, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)k,
+                                                               warps * 32, smem));
+    const int64_t want = div_up(max_count, warps * 32);
+    const unsigned blocks = (unsigned)std::max<int64_t>(
+        1, std::min<int64_t>(want, (int64_t)std::max(per_sm, 1) * h->sm_count));
+    k<<<blocks, warps * 32, smem, h->stream>>>(a, q.env, cands, count, work, key);
+    CDTW_LAUNCH(h, "cdtw_strip_search_kernel");
     return CDTW_OK;
 }
 

@@ -66,6 +66,8 @@ struct cdtw_handle_s {
     bool has_query = false;
     // small pinned host buffer for scalar results
     void* pinned = nullptr;
+    // stage counts of the last search: windows, after LB_Kim, after LB_Keogh
+    int64_t last_counts[4] = {0, 0, 0, 0};
     char err[512] = {0};
 };
 
@@ -138,6 +140,28 @@ __host__ __device__ inline unsigned long long pack_key(float d, uint32_t idx) {
 #endif
 }
 
+// A search candidate: window, its best lower bound, and its forward LB_Keogh
+// (the sum whose suffixes give the cumulative bound for early abandoning).
+struct Cand {
+    int w;
+    float lb;
+    float lbk;
+};
+
+// Lower bounds are compared against the best-so-far with this relative
+// slack, so FP32 rounding of a bound can never prune a window whose distance
+// is below the best (a bound prunes only if it exceeds bsf by 1e-4).
+constexpr float kLbSlack = 1.0f - 1e-4f;
+
+__device__ __forceinline__ float key_dist(unsigned long long k) {
+    return __uint_as_float((unsigned)(k >> 32));
+}
+__device__ __forceinline__ float load_bsf(const unsigned long long* key) {
+    const unsigned long long k = *(const volatile unsigned long long*)key;
+    const float d = key_dist(k);
+    return (k == ~0ull) ? CDTW_INF : d;
+}
+
 // ---- kernel launchers (defined in the .cu files) ----------------------------
 
 int launch_avg_std(cdtw_handle h, const float* x, int64_t N, int M, double* mu, float* sigma);
@@ -150,5 +174,22 @@ int launch_cdtw_strip(cdtw_handle h, const float* x, int64_t N, const double* mu
                       float* out);
 int strip_rows_default(int W);
 int max_register_band();
+int launch_lb_kim(cdtw_handle h, const float* x, int64_t N, const double* mu, const float* sigma,
+                  const int32_t* idx, int64_t L, bool euclid, float* out,
+                  unsigned long long* seeds);
+size_t stream_envelope_scratch_bytes(int64_t N);
+int launch_stream_envelope(cdtw_handle h, const float* x, int64_t N, int W, float* scratch,
+                           float2* env);
+int launch_lb_keogh(cdtw_handle h, const float* x, int64_t N, const double* mu,
+                    const float* sigma, const float2* xenv, const int32_t* idx, int64_t L,
+                    bool euclid, float* fwd, float* rev);
+// DTW over a device candidate list with early abandoning and a fused argmin
+// into *key (packed distance/index).  `count` and `work` are device ints.
+int launch_cdtw_search(cdtw_handle h, const float* x, int64_t N, const double* mu,
+                       const float* sigma, const Cand* cands, const int* count, int* work,
+                       int max_count, bool euclid, unsigned long long* key);
+size_t search_workspace_bytes(int64_t N, int M);
+int run_search(cdtw_handle h, const float* x, int64_t N, const double* mu, const float* sigma,
+               bool euclid, char* ws_base, unsigned long long** key_out, int** ctr_out);
 
 }  // namespace cdtw

@@ -98,6 +98,48 @@ int cdtw_all_windows_host(cdtw_handle h, const float* h_query, int M,
                           const float* h_subject, int64_t N, int W, int metric,
                           float* h_out);
 
+/* ---- lower bounds ------------------------------------------------------------- */
+
+/* LB_Kim of listed windows (all if d_indices == NULL): the reference's 5x5
+ * front + 5x5 back unconstrained-DTW bound on the z-normalised window,
+ * lb_kim (include/bounds.cuh:413-441, kernels :152-407).  Needs M >= 11
+ * (bounds.cuh:418-422); returns CDTW_EINVAL otherwise. */
+int cdtw_lb_kim(cdtw_handle h, const float* d_subject, int64_t N, const double* d_avg,
+                const float* d_std, const int32_t* d_indices, int64_t L, int metric,
+                float* d_out);
+
+/* LB_Keogh of listed windows against the handle query's envelope, lb_keogh
+ * (include/bounds.cuh:443-465, kernel :111-144) -> d_fwd; and the reverse
+ * LB_Keogh of the query against the +-W envelope of the subject
+ * (UCR Suite/UCR_DTW_BIN.cpp:262-282 with the envelope of :607) -> d_rev.
+ * Either output may be NULL. */
+int cdtw_lb_keogh(cdtw_handle h, const float* d_subject, int64_t N, const double* d_avg,
+                  const float* d_std, const int32_t* d_indices, int64_t L, int metric,
+                  float* d_fwd, float* d_rev);
+
+/* ---- pruned search ------------------------------------------------------------- */
+
+/* Best-matching window of the handle's query in the subject: prune_cdtw
+ * (include/cdtw.cuh:510-592) + report_result (:493-508).  *location is the
+ * window start (lowest index on ties, as UCR_DTW_BIN.cpp:682), *distance the
+ * reference's printed "Distance:" (sqrt of the squared cDTW for the Euclidean
+ * cost, the cDTW itself for Manhattan).  LB_Kim -> LB_Keogh / reverse
+ * LB_Keogh -> early-abandoning cDTW, all on the device; one host sync at the
+ * end.  Needs M >= 11. */
+int cdtw_prune_cdtw(cdtw_handle h, const float* d_subject, int64_t N, const double* d_avg,
+                    const float* d_std, int metric, int64_t* location, float* distance);
+
+/* The whole GPU-DTW search from host buffers (GPU-dtw.cu:59-90): H2D of the
+ * subject and query, z-normalisation, statistics, pruned search. */
+int cdtw_search_host(cdtw_handle h, const float* h_query, int M, const float* h_subject,
+                     int64_t N, int W, int metric, int64_t* location, float* distance);
+
+/* Stage counts of the last search on this handle: counts[0] windows,
+ * counts[1] windows below the best-so-far after LB_Kim, counts[2] windows
+ * that reached the cDTW stage.  No reference counterpart (UCR prints the
+ * pruning percentages, UCR_DTW_BIN.cpp:738-741). */
+int cdtw_search_counts(cdtw_handle h, int64_t* counts);
+
 /* ---- fixed-scratch entry point ------------------------------------------------ */
 
 /* Limits of cdtw_all_windows_noalloc and the size of its fixed device array. */
