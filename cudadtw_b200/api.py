@@ -204,3 +204,42 @@ class Handle:
         c = (ctypes.c_int64 * 3)()
         self._check(self._lib.cdtw_search_counts(self._h, c))
         return tuple(c)
+
+    # -- GPU-ED and GPU-LDTW ----------------------------------------------------
+    def ed_all_windows(self, query64, subject64):
+        """Squared z-normalised Euclidean distance per window, FP64
+        (calculate_ed, include/ed.cuh:71-153)."""
+        _dev(query64, torch.float64, "query")
+        _dev(subject64, torch.float64, "subject")
+        out = torch.empty(subject64.numel() - query64.numel() + 1, dtype=torch.float64,
+                          device=subject64.device)
+        self._check(self._lib.ed_all_windows(self._h, _ptr(query64), query64.numel(),
+                                             _ptr(subject64), subject64.numel(), _ptr(out)))
+        return out
+
+    def ed_search_host(self, query, subject):
+        q = np.ascontiguousarray(query, dtype=np.float64)
+        s = np.ascontiguousarray(subject, dtype=np.float64)
+        loc, dist = ctypes.c_int64(), ctypes.c_double()
+        self._check(self._lib.ed_search_host(self._h, _ptr(q), q.size, _ptr(s), s.size,
+                                             ctypes.byref(loc), ctypes.byref(dist)))
+        return loc.value, dist.value
+
+    def ldtw_all_windows(self, subject, metric=EUCLIDEAN):
+        """Greedy LDTW path cost of the query vs every window, FP64
+        (ztsh2_ldtw, include/ldtw.cuh:294-391)."""
+        _dev(subject, torch.float32, "subject")
+        out = torch.empty(subject.numel() - self.M + 1, dtype=torch.float64, device=subject.device)
+        self._check(self._lib.ldtw_all_windows(self._h, _ptr(subject), subject.numel(),
+                                               _metric(metric), _ptr(out)))
+        return out
+
+    def ldtw_search_host(self, query, subject, W, metric=EUCLIDEAN):
+        q = np.ascontiguousarray(query, dtype=np.float32)
+        s = np.ascontiguousarray(subject, dtype=np.float32)
+        loc, dist = ctypes.c_int64(), ctypes.c_double()
+        self._check(self._lib.ldtw_search_host(self._h, _ptr(q), q.size, _ptr(s), s.size, W,
+                                               _metric(metric), ctypes.byref(loc),
+                                               ctypes.byref(dist)))
+        self.M, self.W = q.size, min(W, q.size - 1)
+        return loc.value, dist.value

@@ -357,6 +357,133 @@ int cdtw_search_host(cdtw_handle h, const float* h_query, int M, const float* h_
     return finish_search(h, key, ctr, Nw, metric == CDTW_EUCLIDEAN, location, distance);
 }
 
+// ---- GPU-ED -------------------------------------------------------------------
+
+static int ed_run(cdtw_handle h, const double* dq, int M, const double* dx, int64_t N,
+                  double* dout, char* base, size_t* used) {
+    const int64_t Nw = N - M + 1;
+    Carver c;
+    c.off = *used;
+    const size_t o_zq = c.take<double>(M);
+    const size_t o_mu = c.take<double>(Nw);
+    const size_t o_sd = c.take<double>(Nw);
+    *used = c.off;
+    if (!base) return CDTW_OK;
+    double* zq = (double*)(base + o_zq);
+    double* mu = (double*)(base + o_mu);
+    double* sd = (double*)(base + o_sd);
+    CDTW_TRY(launch_znorm64(h, dq, M, zq));
+    CDTW_TRY(launch_avg_std64(h, dx, N, M, mu, sd));
+    return launch_ed(h, dx, N, zq, M, sd, dout);
+}
+
+int ed_all_windows(cdtw_handle h, const double* d_query, int M, const double* d_subject,
+                   int64_t N, double* d_out) {
+    if (!h) return CDTW_EINVAL;
+    if (!d_query || !d_subject || !d_out) return set_error(h, CDTW_EINVAL, "null pointer");
+    if (M < 1 || M > CDTW_MAX_QUERY || N < M)
+        return set_error(h, CDTW_EINVAL, "need 1 <= M <= min(N, %d)", CDTW_MAX_QUERY);
+    CDTW_CUDA(h, cudaSetDevice(h->device));
+    size_t used = 0;
+    ed_run(h, d_query, M, d_subject, N, d_out, nullptr, &used);
+    CDTW_TRY(ensure_workspace(h, used));
+    used = 0;
+    return ed_run(h, d_query, M, d_subject, N, d_out, (char*)h->ws, &used);
+}
+
+int ed_search_host(cdtw_handle h, const double* h_query, int M, const double* h_subject,
+                   int64_t N, int64_t* location, double* distance) {
+    if (!h) return CDTW_EINVAL;
+    if (!h_query || !h_subject) return set_error(h, CDTW_EINVAL, "null pointer");
+    if (M < 1 || M > CDTW_MAX_QUERY || N < M)
+        return set_error(h, CDTW_EINVAL, "need 1 <= M <= min(N, %d)", CDTW_MAX_QUERY);
+    CDTW_CUDA(h, cudaSetDevice(h->device));
+    const int64_t Nw = N - M + 1;
+    Carver c;
+    const size_t o_q = c.take<double>(M);
+    const size_t o_x = c.take<double>(N);
+    const size_t o_d = c.take<double>(Nw);
+    const size_t o_p = c.take<ArgMin64>(argmin64_partials(Nw));
+    const size_t o_r = c.take<ArgMin64>(1);
+    size_t used = c.off;
+    ed_run(h, nullptr, M, nullptr, N, nullptr, nullptr, &used);
+    CDTW_TRY(ensure_workspace(h, used));
+    char* base = (char*)h->ws;
+    CDTW_CUDA(h, cudaMemcpyAsync(base + o_q, h_query, sizeof(double) * M, cudaMemcpyHostToDevice,
+                                 h->stream));
+    CDTW_CUDA(h, cudaMemcpyAsync(base + o_x, h_subject, sizeof(double) * N,
+                                 cudaMemcpyHostToDevice, h->stream));
+    used = c.off;
+    CDTW_TRY(ed_run(h, (double*)(base + o_q), M, (double*)(base + o_x), N,
+                    (double*)(base + o_d), base, &used));
+    CDTW_TRY(launch_argmin64(h, (double*)(base + o_d), Nw, (ArgMin64*)(base + o_p),
+                             (ArgMin64*)(base + o_r)));
+    ArgMin64* pin = (ArgMin64*)h->pinned;
+    CDTW_CUDA(h, cudaMemcpyAsync(pin, base + o_r, sizeof(ArgMin64), cudaMemcpyDeviceToHost,
+                                 h->stream));
+    CDTW_CUDA(h, cudaStreamSynchronize(h->stream));
+    if (location) *location = pin->i;
+    if (distance) *distance = sqrt(fmax(pin->v, 0.0));
+    return CDTW_OK;
+}
+
+// ---- GPU-LDTW -----------------------------------------------------------------
+
+int ldtw_all_windows(cdtw_handle h, const float* d_subject, int64_t N, int metric,
+                     double* d_out) {
+    if (!h) return CDTW_EINVAL;
+    if (!h->has_query) return set_error(h, CDTW_EINVAL, "no query set (cdtw_set_query)");
+    if (!d_subject || !d_out) return set_error(h, CDTW_EINVAL, "null pointer");
+    if (!valid_metric(metric)) return set_error(h, CDTW_EINVAL, "bad metric %d", metric);
+    const int M = h->q.M;
+    if (N < M) return set_error(h, CDTW_EINVAL, "subject shorter than query");
+    CDTW_CUDA(h, cudaSetDevice(h->device));
+    const int64_t Nw = N - M + 1;
+    Carver c;
+    const size_t o_mu = c.take<double>(Nw);
+    const size_t o_sd = c.take<double>(Nw);
+    CDTW_TRY(ensure_workspace(h, c.off));
+    char* base = (char*)h->ws;
+    CDTW_TRY(launch_avg_std64(h, d_subject, N, M, (double*)(base + o_mu), (double*)(base + o_sd)));
+    return launch_ldtw(h, d_subject, N, (double*)(base + o_mu), (double*)(base + o_sd),
+                       metric == CDTW_EUCLIDEAN, d_out);
+}
+
+int ldtw_search_host(cdtw_handle h, const float* h_query, int M, const float* h_subject,
+                     int64_t N, int W, int metric, int64_t* location, double* distance) {
+    if (!h) return CDTW_EINVAL;
+    if (!h_query || !h_subject) return set_error(h, CDTW_EINVAL, "null pointer");
+    if (!valid_metric(metric)) return set_error(h, CDTW_EINVAL, "bad metric %d", metric);
+    if (M < 1 || N < M) return set_error(h, CDTW_EINVAL, "need 1 <= M <= N");
+    CDTW_CUDA(h, cudaSetDevice(h->device));
+    const int64_t Nw = N - M + 1;
+    Carver c;
+    const size_t o_x = c.take<float>(N);
+    const size_t o_mu = c.take<double>(Nw);
+    const size_t o_sd = c.take<double>(Nw);
+    const size_t o_d = c.take<double>(Nw);
+    const size_t o_p = c.take<ArgMin64>(argmin64_partials(Nw));
+    const size_t o_r = c.take<ArgMin64>(1);
+    CDTW_TRY(ensure_workspace(h, c.off));
+    char* base = (char*)h->ws;
+    float* dx = (float*)(base + o_x);
+    CDTW_CUDA(h, cudaMemcpyAsync(dx, h_subject, sizeof(float) * N, cudaMemcpyHostToDevice,
+                                 h->stream));
+    CDTW_TRY(cdtw_set_query(h, h_query, M, W, CDTW_HOST));
+    CDTW_TRY(launch_avg_std64(h, dx, N, M, (double*)(base + o_mu), (double*)(base + o_sd)));
+    CDTW_TRY(launch_ldtw(h, dx, N, (double*)(base + o_mu), (double*)(base + o_sd),
+                         metric == CDTW_EUCLIDEAN, (double*)(base + o_d)));
+    CDTW_TRY(launch_argmin64(h, (double*)(base + o_d), Nw, (ArgMin64*)(base + o_p),
+                             (ArgMin64*)(base + o_r)));
+    ArgMin64* pin = (ArgMin64*)h->pinned;
+    CDTW_CUDA(h, cudaMemcpyAsync(pin, base + o_r, sizeof(ArgMin64), cudaMemcpyDeviceToHost,
+                                 h->stream));
+    CDTW_CUDA(h, cudaStreamSynchronize(h->stream));
+    if (location) *location = pin->i;
+    if (distance) *distance = metric == CDTW_EUCLIDEAN ? sqrt(pin->v) : pin->v;
+    return CDTW_OK;
+}
+
 int cdtw_search_counts(cdtw_handle h, int64_t* counts) {
     if (!h || !counts) return CDTW_EINVAL;
     for (int i = 0; i < 3; ++i) counts[i] = h->last_counts[i];

@@ -165,6 +165,22 @@ __device__ __forceinline__ float load_bsf(const unsigned long long* key) {
 // ---- kernel launchers (defined in the .cu files) ----------------------------
 
 int launch_avg_std(cdtw_handle h, const float* x, int64_t N, int M, double* mu, float* sigma);
+int launch_avg_std64(cdtw_handle h, const float* x, int64_t N, int M, double* mu, double* sigma);
+int launch_avg_std64(cdtw_handle h, const double* x, int64_t N, int M, double* mu, double* sigma);
+// Exact FP64 argmin (lowest index on ties) of d[0..n): block partials then one
+// final block; the result (value, index) lands in *res.
+struct ArgMin64 {
+    double v;
+    long long i;
+};
+int launch_argmin64(cdtw_handle h, const double* d, int64_t n, ArgMin64* partial,
+                    ArgMin64* res);
+size_t argmin64_partials(int64_t n);
+int launch_znorm64(cdtw_handle h, const double* q, int M, double* zq);
+int launch_ed(cdtw_handle h, const double* x, int64_t N, const double* zq, int M,
+              const double* sigma, double* out);
+int launch_ldtw(cdtw_handle h, const float* x, int64_t N, const double* mu, const double* sigma,
+                bool euclid, double* out);
 int launch_prepare_query(cdtw_handle h, const float* d_query_raw, int M, int W);
 int launch_cdtw_windows(cdtw_handle h, const float* x, int64_t N, const double* mu,
                         const float* sigma, const int32_t* idx, int64_t L, bool euclid,

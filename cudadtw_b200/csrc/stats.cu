@@ -33,9 +33,10 @@ __device__ __forceinline__ double warp_incl_scan(double v, int lane) {
     return v;
 }
 
+template <class XT, class ST>
 __global__ void __launch_bounds__(kStatsBlock)
-avg_std_kernel(const float* __restrict__ x, int64_t N, int M, double* __restrict__ mu,
-               float* __restrict__ sigma) {
+avg_std_kernel(const XT* __restrict__ x, int64_t N, int M, double* __restrict__ mu,
+               ST* __restrict__ sigma) {
     const int64_t Nw = N - M + 1;
     const int lane = threadIdx.x & 31;
     const int64_t warp = (int64_t)blockIdx.x * (kStatsBlock / 32) + (threadIdx.x >> 5);
@@ -69,7 +70,7 @@ avg_std_kernel(const float* __restrict__ x, int64_t N, int M, double* __restrict
             const double m1 = w1 * invM;
             const double var = w2 * invM - m1 * m1;
             mu[w] = c + m1;
-            sigma[w] = var > 0.0 ? (float)sqrt(var) : 1.0f;
+            sigma[w] = var > 0.0 ? (ST)sqrt(var) : (ST)1;
         }
         s1 += __shfl_sync(0xffffffffu, i1, 31);
         s2 += __shfl_sync(0xffffffffu, i2, 31);
@@ -154,7 +155,24 @@ int launch_avg_std(cdtw_handle h, const float* x, int64_t N, int M, double* mu, 
     const int64_t Nw = N - M + 1;
     const int64_t warps = div_up(Nw, kStatsWarpWindows);
     const int64_t blocks = div_up(warps, kStatsBlock / 32);
-    avg_std_kernel<<<(unsigned)blocks, kStatsBlock, 0, h->stream>>>(x, N, M, mu, sigma);
+    avg_std_kernel<float, float><<<(unsigned)blocks, kStatsBlock, 0, h->stream>>>(x, N, M, mu,
+                                                                                  sigma);
+    CDTW_LAUNCH(h, "avg_std_kernel");
+    return CDTW_OK;
+}
+
+// FP64 sigma (ED and LDTW paths), float32 or float64 series.
+int launch_avg_std64(cdtw_handle h, const float* x, int64_t N, int M, double* mu, double* sigma) {
+    const int64_t blocks = div_up(div_up(N - M + 1, kStatsWarpWindows), kStatsBlock / 32);
+    avg_std_kernel<float, double><<<(unsigned)blocks, kStatsBlock, 0, h->stream>>>(x, N, M, mu,
+                                                                                   sigma);
+    CDTW_LAUNCH(h, "avg_std_kernel");
+    return CDTW_OK;
+}
+int launch_avg_std64(cdtw_handle h, const double* x, int64_t N, int M, double* mu, double* sigma) {
+    const int64_t blocks = div_up(div_up(N - M + 1, kStatsWarpWindows), kStatsBlock / 32);
+    avg_std_kernel<double, double><<<(unsigned)blocks, kStatsBlock, 0, h->stream>>>(x, N, M, mu,
+                                                                                    sigma);
     CDTW_LAUNCH(h, "avg_std_kernel");
     return CDTW_OK;
 }

@@ -140,6 +140,35 @@ int cdtw_search_host(cdtw_handle h, const float* h_query, int M, const float* h_
  * pruning percentages, UCR_DTW_BIN.cpp:738-741). */
 int cdtw_search_counts(cdtw_handle h, int64_t* counts);
 
+/* ---- GPU-ED: z-normalised Euclidean distance (float64) --------------------------- */
+
+/* Squared z-normalised Euclidean distance of the query to every window,
+ * d_out[w] = 2M - 2*corr(w)/sigma_w = sum_k (zq_k - z_k)^2, in FP64:
+ * calculate_ed (include/ed.cuh:71-153) without the FFT and the argsort.
+ * The raw float64 query is z-normalised on the device. */
+int ed_all_windows(cdtw_handle h, const double* d_query, int M, const double* d_subject,
+                   int64_t N, double* d_out);
+
+/* The whole GPU-ED search from host buffers (GPU-ed.cu:51-82): *location is
+ * the best window (lowest on ties), *distance = sqrt(min d^2), the
+ * reference's "distance:" line (ed.cuh:323). */
+int ed_search_host(cdtw_handle h, const double* h_query, int M, const double* h_subject,
+                   int64_t N, int64_t* location, double* distance);
+
+/* ---- GPU-LDTW: greedy local path in the band ---------------------------------- */
+
+/* Cost of the greedy locally-optimal warping path of the handle's query
+ * (cdtw_set_query, band W) against every window, FP64: ztsh2_ldtw
+ * (include/ldtw.cuh:294-391), tie rule of ldtw.cuh:368-383. */
+int ldtw_all_windows(cdtw_handle h, const float* d_subject, int64_t N, int metric,
+                     double* d_out);
+
+/* The whole GPU-LDTW search from host buffers (GPU-ldtw.cu:44-98): first
+ * strict minimum (determine_min, ldtw.cuh:177-192); *distance = sqrt of the
+ * path cost for the Euclidean cost. */
+int ldtw_search_host(cdtw_handle h, const float* h_query, int M, const float* h_subject,
+                     int64_t N, int W, int metric, int64_t* location, double* distance);
+
 /* ---- fixed-scratch entry point ------------------------------------------------ */
 
 /* Limits of cdtw_all_windows_noalloc and the size of its fixed device array. */

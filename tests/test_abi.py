@@ -37,3 +37,22 @@ def test_create_without_gpu_fails_cleanly():
     h = ctypes.c_void_p()
     st = lib.cdtw_create(ctypes.byref(h), 0)
     assert st in (1, 3) and not h.value
+
+
+def test_drivers_usage_and_argument_checks_without_gpu():
+    """The drop-in drivers keep the reference's usage line and return 1 on
+    bad arguments before touching a GPU."""
+    import os
+    import subprocess
+    d = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))),
+                     "cudadtw_b200", "drivers")
+    for name, nargs in (("GPU-DTW", 5), ("GPU-ED", 4), ("GPU-LDTW", 5)):
+        exe = os.path.join(d, name)
+        if not os.path.exists(exe):
+            continue
+        r = subprocess.run([exe], capture_output=True, text=True)
+        assert r.returncode == 1 and r.stdout.startswith("call")
+    exe = os.path.join(d, "GPU-DTW")
+    if os.path.exists(exe):
+        r = subprocess.run([exe, "q", "s", "8", "100", "10"], capture_output=True, text=True)
+        assert r.returncode == 1 and "window = 0" in r.stdout  # M < 11 refused

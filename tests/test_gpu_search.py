@@ -132,3 +132,15 @@ def test_search_with_constant_windows(handle):
     loc, dist = handle.prune_cdtw(dx, avg, std)
     allw = handle.gpu_cdtw(dx, avg, std).cpu().numpy()
     assert loc == int(np.argmin(allw))
+
+
+def test_search_config0_full_size_equals_unpruned(handle):
+    """The 2^20-sample ECG-like configuration: pruned search == argmin of the
+    unpruned all-windows cDTW, for W=12 (10%) and W=13."""
+    x = synth.ecg_like(1 << 20, seed=0)
+    q, _ = synth.cut_query(x, 128, seed=12810, noise=0.05)
+    for w in (12, 13):
+        dx, avg, std = _prep(handle, q, x, w)
+        loc, dist = handle.prune_cdtw(dx, avg, std)
+        allw = handle.gpu_cdtw(dx, avg, std).cpu().numpy()
+        assert loc == int(np.argmin(allw)) and dist == np.float32(np.sqrt(allw.min()))
