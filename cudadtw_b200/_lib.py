@@ -34,6 +34,7 @@ SIGNATURES = {
     "cdtw_prune_cdtw": (c_int, [c_vp, c_vp, c_i64, c_vp, c_vp, c_int, c_i64p, c_f32p]),
     "cdtw_search_host": (c_int, [c_vp, c_vp, c_int, c_vp, c_i64, c_int, c_int, c_i64p, c_f32p]),
     "cdtw_search_counts": (c_int, [c_vp, c_i64p]),
+    "cdtw_set_band_variant": (c_int, [c_vp, c_int, c_int, c_int]),
     "ed_all_windows": (c_int, [c_vp, c_vp, c_int, c_vp, c_i64, c_vp]),
     "ed_search_host": (c_int, [c_vp, c_vp, c_int, c_vp, c_i64, c_i64p, c_f64p]),
     "ldtw_all_windows": (c_int, [c_vp, c_vp, c_i64, c_int, c_vp]),

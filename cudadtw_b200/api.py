@@ -243,3 +243,11 @@ class Handle:
                                                ctypes.byref(dist)))
         self.M, self.W = q.size, min(W, q.size - 1)
         return loc.value, dist.value
+
+    # -- kernel selection -----------------------------------------------------
+    VARIANTS = {"auto": 0, "register": 1, "strip16": 2, "strip32": 3}
+
+    def set_band_variant(self, w_lo: int, w_hi: int, variant) -> None:
+        """cDTW kernel variant for bands w_lo..w_hi (the autotuner's knob)."""
+        v = self.VARIANTS[variant] if isinstance(variant, str) else int(variant)
+        self._check(self._lib.cdtw_set_band_variant(self._h, w_lo, w_hi, v))

@@ -153,6 +153,7 @@ int cdtw_destroy(cdtw_handle h) {
     cudaStreamSynchronize(h->stream);
     if (h->ws) cudaFree(h->ws);
     if (h->qmem) cudaFree(h->qmem);
+    if (h->ring) cudaFree(h->ring);
     if (h->pinned) cudaFreeHost(h->pinned);
     if (h->own_stream) cudaStreamDestroy(h->own_stream);
     delete h;
@@ -481,6 +482,14 @@ int ldtw_search_host(cdtw_handle h, const float* h_query, int M, const float* h_
     CDTW_CUDA(h, cudaStreamSynchronize(h->stream));
     if (location) *location = pin->i;
     if (distance) *distance = metric == CDTW_EUCLIDEAN ? sqrt(pin->v) : pin->v;
+    return CDTW_OK;
+}
+
+int cdtw_set_band_variant(cdtw_handle h, int w_lo, int w_hi, int variant) {
+    if (!h) return CDTW_EINVAL;
+    if (variant < CDTW_VARIANT_AUTO || variant > CDTW_VARIANT_STRIP32 || w_lo < 0 || w_hi < w_lo)
+        return set_error(h, CDTW_EINVAL, "bad band range or variant");
+    for (int w = w_lo; w <= w_hi && w < CDTW_MAX_QUERY; ++w) h->band_variant[w] = (unsigned char)variant;
     return CDTW_OK;
 }
 

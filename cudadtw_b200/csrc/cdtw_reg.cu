@@ -16,196 +16,11 @@
 // [0, M) are padded with +inf, which makes out-of-matrix cells +inf without
 // any per-cell test.  The result D[M-1][W] equals the reference's
 // penalty[...][M] (cdtw.cuh:83).
-#include "common.cuh"
-
-#include <algorithm>
+#include "cdtw_reg.cuh"
 
 namespace cdtw {
 
 namespace {
-
-constexpr int kRegBlock = 128;
-constexpr int kMaxRegW = 40;
-
-template <int W, bool EU>
-__global__ void __launch_bounds__(kRegBlock)
-cdtw_reg_kernel(const float* __restrict__ x, const double* __restrict__ mu,
-                const float* __restrict__ sigma, const float4* __restrict__ qpad4, int lq4,
-                int M, int Nw, const int32_t* __restrict__ idx, int L, float* __restrict__ out) {
-    extern __shared__ float4 sq4[];
-    for (int e = threadIdx.x; e < 4 * lq4; e += blockDim.x) sq4[e] = qpad4[e];
-    __syncthreads();
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= L) return;
-    const int w = idx ? idx[t] : t;
-    if (w < 0 || w >= Nw) {  // a listed window outside the subject: NaN, no access
-        out[t] = __int_as_float(0x7fc00000);
-        return;
-    }
-    const Norm nm = make_norm(mu[w], sigma[w]);
-    const float* __restrict__ xw = x + w;
-
-    constexpr int B = 2 * W + 1;
-    constexpr int NQ4 = (B + 3) / 4;
-    float prev[B + 1];
-#pragma unroll
-    for (int k = 0; k <= B; ++k) prev[k] = CDTW_INF;
-    prev[W] = 0.0f;  // virtual D[-1][-1] = 0 (cdtw.cuh:35, :191)
-    float res = CDTW_INF;
-
-    for (int j0 = 0; j0 < M; j0 += 4) {
-#pragma unroll
-        for (int u = 0; u < 4; ++u) {
-            const int j = j0 + u;
-            const float z = znorm(nm, __ldg(xw + min(j, M - 1)));
-            const float4* qr = sq4 + u * lq4 + (j0 >> 2);
-            float qv[NQ4 * 4];
-#pragma unroll
-            for (int r = 0; r < NQ4; ++r) {
-                const float4 v = qr[r];
-                qv[4 * r + 0] = v.x;
-                qv[4 * r + 1] = v.y;
-                qv[4 * r + 2] = v.z;
-                qv[4 * r + 3] = v.w;
-            }
-            float left = CDTW_INF;
-            float cur[B];
-#pragma unroll
-            for (int k = 0; k < B; ++k) {
-                const float m = min3f(prev[k], prev[k + 1], left);
-                left = cell<EU>(z - qv[k], m);
-                cur[k] = left;
-            }
-            if (j == M - 1) res = cur[W];
-#pragma unroll
-            for (int k = 0; k < B; ++k) prev[k] = cur[k];
-        }
-    }
-    out[t] = res;
-}
-
-// Search variant: persistent warps take 32 candidates at a time from a device
-// list, skip those whose lower bound already exceeds the best-so-far, run the
-// register-band DTW, and abandon a candidate once its last row minimum plus
-// the remaining suffix of its forward LB_Keogh (the cumulative bound cb of
-// UCR_DTW_BIN.cpp:666-677, :336) reaches the best-so-far.  The warp leaves a
-// group when all 32 lanes have abandoned.  Results fold into *key by a packed
-// (distance, window) atomicMin, so ties keep the lowest window.
-template <int W, bool EU>
-__global__ void __launch_bounds__(kRegBlock)
-cdtw_reg_search_kernel(const float* __restrict__ x, const double* __restrict__ mu,
-                       const float* __restrict__ sigma, const float4* __restrict__ qpad4, int lq4,
-                       const float2* __restrict__ qenv, int M, const Cand* __restrict__ cands,
-                       const int* __restrict__ count, int* __restrict__ work,
-                       unsigned long long* __restrict__ key) {
-    extern __shared__ float4 sq4[];
-    float2* senv = (float2*)(sq4 + 4 * lq4);
-    for (int e = threadIdx.x; e < 4 * lq4; e += blockDim.x) sq4[e] = qpad4[e];
-    for (int e = threadIdx.x; e < M; e += blockDim.x) senv[e] = qenv[e];
-    __syncthreads();
-    const int lane = threadIdx.x & 31;
-    const int n = *(const volatile int*)count;
-    constexpr int B = 2 * W + 1;
-    constexpr int NQ4 = (B + 3) / 4;
-    for (;;) {
-        int base = 0;
-        if (lane == 0) base = atomicAdd(work, 32);
-        base = __shfl_sync(0xffffffffu, base, 0);
-        if (base >= n) break;
-        const int i = base + lane;
-        Cand c;
-        c.w = 0;
-        c.lb = CDTW_INF;
-        c.lbk = 0.f;
-        if (i < n) c = cands[i];
-        float bsf = load_bsf(key);
-        bool alive = (i < n) && (c.lb * kLbSlack < bsf);
-        if (!__any_sync(0xffffffffu, alive)) continue;
-        const int w = c.w;
-        const Norm nm = make_norm(mu[w], sigma[w]);
-        const float* __restrict__ xw = x + w;
-        float prev[B + 1];
-#pragma unroll
-        for (int k = 0; k <= B; ++k) prev[k] = CDTW_INF;
-        prev[W] = 0.0f;
-        float res = CDTW_INF, pre = 0.f;
-        for (int j0 = 0; j0 < M; j0 += 4) {
-#pragma unroll
-            for (int u = 0; u < 4; ++u) {
-                const int j = j0 + u;
-                const int jc = min(j, M - 1);
-                const float z = znorm(nm, __ldg(xw + jc));
-                // forward LB_Keogh term of this data row (query envelope at j)
-                const float2 e = senv[jc];
-                const float dl = max3f(z - e.y, e.x - z, 0.f);
-                pre += (j < M) ? (EU ? dl * dl : dl) : 0.f;
-                const float4* qr = sq4 + u * lq4 + (j0 >> 2);
-                float qv[NQ4 * 4];
-#pragma unroll
-                for (int r = 0; r < NQ4; ++r) {
-                    const float4 v = qr[r];
-                    qv[4 * r + 0] = v.x;
-                    qv[4 * r + 1] = v.y;
-                    qv[4 * r + 2] = v.z;
-                    qv[4 * r + 3] = v.w;
-                }
-                float left = CDTW_INF;
-                float cur[B];
-#pragma unroll
-                for (int k = 0; k < B; ++k) {
-                    const float m = min3f(prev[k], prev[k + 1], left);
-                    left = cell<EU>(z - qv[k], m);
-                    cur[k] = left;
-                }
-                if (j == M - 1) res = cur[W];
-#pragma unroll
-                for (int k = 0; k < B; ++k) prev[k] = cur[k];
-            }
-            if ((j0 & 7) == 4 && j0 + 3 < M - 1) {  // rows j0..j0+3 are all real rows
-                float rmin = prev[0];
-#pragma unroll
-                for (int k = 1; k < B; k += 2) rmin = min3f(rmin, prev[k], prev[k + 1]);
-                bsf = load_bsf(key);
-                alive = alive && (rmin + (c.lbk - pre) * kLbSlack < bsf);
-                if (!__any_sync(0xffffffffu, alive)) break;
-            }
-        }
-        if (i < n && res < CDTW_INF) atomicMin(key, pack_key(res, (uint32_t)w));
-    }
-}
-
-using RegKernel = void (*)(const float*, const double*, const float*, const float4*, int, int,
-                           int, const int32_t*, int, float*);
-
-template <int W>
-struct RegTable {
-    static void fill(RegKernel* eu, RegKernel* mh) {
-        eu[W] = cdtw_reg_kernel<W, true>;
-        mh[W] = cdtw_reg_kernel<W, false>;
-        RegTable<W - 1>::fill(eu, mh);
-    }
-};
-template <>
-struct RegTable<-1> {
-    static void fill(RegKernel*, RegKernel*) {}
-};
-
-using RegSearchKernel = void (*)(const float*, const double*, const float*, const float4*, int,
-                                 const float2*, int, const Cand*, const int*, int*,
-                                 unsigned long long*);
-
-template <int W>
-struct RegSearchTable {
-    static void fill(RegSearchKernel* eu, RegSearchKernel* mh) {
-        eu[W] = cdtw_reg_search_kernel<W, true>;
-        mh[W] = cdtw_reg_search_kernel<W, false>;
-        RegSearchTable<W - 1>::fill(eu, mh);
-    }
-};
-template <>
-struct RegSearchTable<-1> {
-    static void fill(RegSearchKernel*, RegSearchKernel*) {}
-};
 
 struct RegKernels {
     RegKernel eu[kMaxRegW + 1];
@@ -213,8 +28,16 @@ struct RegKernels {
     RegSearchKernel seu[kMaxRegW + 1];
     RegSearchKernel smh[kMaxRegW + 1];
     RegKernels() {
-        RegTable<kMaxRegW>::fill(eu, mh);
-        RegSearchTable<kMaxRegW>::fill(seu, smh);
+        void** a = (void**)eu;
+        void** b = (void**)mh;
+        void** c = (void**)seu;
+        void** d = (void**)smh;
+        reg_fill_part0(a, b, c, d);
+        reg_fill_part1(a, b, c, d);
+        reg_fill_part2(a, b, c, d);
+        reg_fill_part3(a, b, c, d);
+        reg_fill_part4(a, b, c, d);
+        reg_fill_part5(a, b, c, d);
     }
 };
 
@@ -227,6 +50,15 @@ const RegKernels& reg_kernels() {
 
 int max_register_band() { return kMaxRegW; }
 
+int choose_variant(cdtw_handle h, int W) {
+    int v = (W >= 0 && W < CDTW_MAX_QUERY) ? h->band_variant[W] : 0;
+    if (v == CDTW_VARIANT_REGISTER && W > kMaxRegW) v = 0;
+    if (v == CDTW_VARIANT_STRIP16 && W < 15) v = 0;
+    if (v == CDTW_VARIANT_STRIP32 && W < 31) v = 0;
+    if (v == 0) v = (W <= kMaxRegW) ? CDTW_VARIANT_REGISTER : CDTW_VARIANT_STRIP16;
+    return v;
+}
+
 int launch_cdtw_strip_search(cdtw_handle h, const float* x, int64_t N, const double* mu,
                              const float* sigma, const Cand* cands, const int* count, int* work,
                              int max_count, bool euclid, int R, unsigned long long* key);
@@ -236,9 +68,10 @@ int launch_cdtw_search(cdtw_handle h, const float* x, int64_t N, const double* m
                        int max_count, bool euclid, unsigned long long* key) {
     const QueryPack& q = h->q;
     if (max_count <= 0) return CDTW_OK;
-    if (q.W > kMaxRegW)
+    const int variant = choose_variant(h, q.W);
+    if (variant != CDTW_VARIANT_REGISTER)
         return launch_cdtw_strip_search(h, x, N, mu, sigma, cands, count, work, max_count,
-                                        euclid, strip_rows_default(q.W), key);
+                                        euclid, variant == CDTW_VARIANT_STRIP16 ? 16 : 32, key);
     RegSearchKernel k = euclid ? reg_kernels().seu[q.W] : reg_kernels().smh[q.W];
     const int lq4 = q.lq / 4;
     const size_t smem = (size_t)q.lq * 4 * sizeof(float) + (size_t)q.M * sizeof(float2);
@@ -261,12 +94,13 @@ int launch_cdtw_windows(cdtw_handle h, const float* x, int64_t N, const double* 
                         float* out) {
     const QueryPack& q = h->q;
     const int Nw = (int)(N - q.M + 1);
-    if (q.W > kMaxRegW) {
+    const int variant = q.qrev ? choose_variant(h, q.W) : CDTW_VARIANT_REGISTER;
+    if (variant != CDTW_VARIANT_REGISTER || q.W > kMaxRegW) {
         if (!q.qrev)
             return set_error(h, CDTW_EUNSUPPORTED, "band W=%d above the register-band limit %d",
                              q.W, kMaxRegW);
-        return launch_cdtw_strip(h, x, N, mu, sigma, idx, L, euclid, strip_rows_default(q.W),
-                                 out);
+        return launch_cdtw_strip(h, x, N, mu, sigma, idx, L, euclid,
+                                 variant == CDTW_VARIANT_STRIP16 ? 16 : 32, out);
     }
     if (L <= 0) return CDTW_OK;
     RegKernel k = euclid ? reg_kernels().eu[q.W] : reg_kernels().mh[q.W];

@@ -1,0 +1,209 @@
+// Banded DTW with the whole band of one window in registers ("register band").
+//
+// Reference: sparse_block_cdtw / dense_block_cdtw (include/cdtw.cuh:164-363),
+// which spread one window over W+2 threads and step the anti-diagonals through
+// shared memory with a __syncthreads per step.  Windows are independent and
+// there are millions of them, so here one thread owns one window and keeps
+// the 2W+1 band cells of the current row in registers; the 32 lanes of a warp
+// run 32 neighbouring windows in lockstep, so all lanes read the same query
+// values (a shared-memory broadcast) and consecutive stream samples (one
+// coalesced 128-byte load per row).
+//
+// Orientation: rows are window (data) positions j = 0..M-1, columns are query
+// positions i, band coordinate k = i - j + W in [0, 2W].  The cell update
+//   D[j][k] = cost(z_j, q_{j-W+k}) + min(D[j-1][k], D[j-1][k+1], D[j][k-1])
+// is one FADD, one three-input FMNMX and one FFMA.  Query positions outside
+// [0, M) are padded with +inf, which makes out-of-matrix cells +inf without
+// any per-cell test.  The result D[M-1][W] equals the reference's
+// penalty[...][M] (cdtw.cuh:83).
+#pragma once
+
+#include "common.cuh"
+
+#include <algorithm>
+
+namespace cdtw {
+
+namespace {
+
+constexpr int kRegBlock = 128;
+constexpr int kMaxRegW = 96;
+
+template <int W, bool EU>
+__global__ void __launch_bounds__(kRegBlock)
+cdtw_reg_kernel(const float* __restrict__ x, const double* __restrict__ mu,
+                const float* __restrict__ sigma, const float4* __restrict__ qpad4, int lq4,
+                int M, int Nw, const int32_t* __restrict__ idx, int L, float* __restrict__ out) {
+    extern __shared__ float4 sq4[];
+    for (int e = threadIdx.x; e < 4 * lq4; e += blockDim.x) sq4[e] = qpad4[e];
+    __syncthreads();
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= L) return;
+    const int w = idx ? idx[t] : t;
+    if (w < 0 || w >= Nw) {  // a listed window outside the subject: NaN, no access
+        out[t] = __int_as_float(0x7fc00000);
+        return;
+    }
+    const Norm nm = make_norm(mu[w], sigma[w]);
+    const float* __restrict__ xw = x + w;
+
+    constexpr int B = 2 * W + 1;
+    constexpr int NQ4 = (B + 3) / 4;
+    float prev[B + 1];
+#pragma unroll
+    for (int k = 0; k <= B; ++k) prev[k] = CDTW_INF;
+    prev[W] = 0.0f;  // virtual D[-1][-1] = 0 (cdtw.cuh:35, :191)
+    float res = CDTW_INF;
+
+    for (int j0 = 0; j0 < M; j0 += 4) {
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int j = j0 + u;
+            const float z = znorm(nm, __ldg(xw + min(j, M - 1)));
+            const float4* qr = sq4 + u * lq4 + (j0 >> 2);
+            float qv[NQ4 * 4];
+#pragma unroll
+            for (int r = 0; r < NQ4; ++r) {
+                const float4 v = qr[r];
+                qv[4 * r + 0] = v.x;
+                qv[4 * r + 1] = v.y;
+                qv[4 * r + 2] = v.z;
+                qv[4 * r + 3] = v.w;
+            }
+            float left = CDTW_INF;
+            float cur[B];
+#pragma unroll
+            for (int k = 0; k < B; ++k) {
+                const float m = min3f(prev[k], prev[k + 1], left);
+                left = cell<EU>(z - qv[k], m);
+                cur[k] = left;
+            }
+            if (j == M - 1) res = cur[W];
+#pragma unroll
+            for (int k = 0; k < B; ++k) prev[k] = cur[k];
+        }
+    }
+    out[t] = res;
+}
+
+// Search variant: persistent warps take 32 candidates at a time from a device
+// list, skip those whose lower bound already exceeds the best-so-far, run the
+// register-band DTW, and abandon a candidate once its last row minimum plus
+// the remaining suffix of its forward LB_Keogh (the cumulative bound cb of
+// UCR_DTW_BIN.cpp:666-677, :336) reaches the best-so-far.  The warp leaves a
+// group when all 32 lanes have abandoned.  Results fold into *key by a packed
+// (distance, window) atomicMin, so ties keep the lowest window.
+template <int W, bool EU>
+__global__ void __launch_bounds__(kRegBlock)
+cdtw_reg_search_kernel(const float* __restrict__ x, const double* __restrict__ mu,
+                       const float* __restrict__ sigma, const float4* __restrict__ qpad4, int lq4,
+                       const float2* __restrict__ qenv, int M, const Cand* __restrict__ cands,
+                       const int* __restrict__ count, int* __restrict__ work,
+                       unsigned long long* __restrict__ key) {
+    extern __shared__ float4 sq4[];
+    float2* senv = (float2*)(sq4 + 4 * lq4);
+    for (int e = threadIdx.x; e < 4 * lq4; e += blockDim.x) sq4[e] = qpad4[e];
+    for (int e = threadIdx.x; e < M; e += blockDim.x) senv[e] = qenv[e];
+    __syncthreads();
+    const int lane = threadIdx.x & 31;
+    const int n = *(const volatile int*)count;
+    constexpr int B = 2 * W + 1;
+    constexpr int NQ4 = (B + 3) / 4;
+    for (;;) {
+        int base = 0;
+        if (lane == 0) base = atomicAdd(work, 32);
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (base >= n) break;
+        const int i = base + lane;
+        Cand c;
+        c.w = 0;
+        c.lb = CDTW_INF;
+        c.lbk = 0.f;
+        if (i < n) c = cands[i];
+        float bsf = load_bsf(key);
+        bool alive = (i < n) && (c.lb * kLbSlack < bsf);
+        if (!__any_sync(0xffffffffu, alive)) continue;
+        const int w = c.w;
+        const Norm nm = make_norm(mu[w], sigma[w]);
+        const float* __restrict__ xw = x + w;
+        float prev[B + 1];
+#pragma unroll
+        for (int k = 0; k <= B; ++k) prev[k] = CDTW_INF;
+        prev[W] = 0.0f;
+        float res = CDTW_INF, pre = 0.f;
+        for (int j0 = 0; j0 < M; j0 += 4) {
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int j = j0 + u;
+                const int jc = min(j, M - 1);
+                const float z = znorm(nm, __ldg(xw + jc));
+                // forward LB_Keogh term of this data row (query envelope at j)
+                const float2 e = senv[jc];
+                const float dl = max3f(z - e.y, e.x - z, 0.f);
+                pre += (j < M) ? (EU ? dl * dl : dl) : 0.f;
+                const float4* qr = sq4 + u * lq4 + (j0 >> 2);
+                float qv[NQ4 * 4];
+#pragma unroll
+                for (int r = 0; r < NQ4; ++r) {
+                    const float4 v = qr[r];
+                    qv[4 * r + 0] = v.x;
+                    qv[4 * r + 1] = v.y;
+                    qv[4 * r + 2] = v.z;
+                    qv[4 * r + 3] = v.w;
+                }
+                float left = CDTW_INF;
+                float cur[B];
+#pragma unroll
+                for (int k = 0; k < B; ++k) {
+                    const float m = min3f(prev[k], prev[k + 1], left);
+                    left = cell<EU>(z - qv[k], m);
+                    cur[k] = left;
+                }
+                if (j == M - 1) res = cur[W];
+#pragma unroll
+                for (int k = 0; k < B; ++k) prev[k] = cur[k];
+            }
+            if ((j0 & 7) == 4 && j0 + 3 < M - 1) {  // rows j0..j0+3 are all real rows
+                float rmin = prev[0];
+#pragma unroll
+                for (int k = 1; k < B; k += 2) rmin = min3f(rmin, prev[k], prev[k + 1]);
+                bsf = load_bsf(key);
+                alive = alive && (rmin + (c.lbk - pre) * kLbSlack < bsf);
+                if (!__any_sync(0xffffffffu, alive)) break;
+            }
+        }
+        if (i < n && res < CDTW_INF) atomicMin(key, pack_key(res, (uint32_t)w));
+    }
+}
+
+using RegKernel = void (*)(const float*, const double*, const float*, const float4*, int, int,
+                           int, const int32_t*, int, float*);
+using RegSearchKernel = void (*)(const float*, const double*, const float*, const float4*, int,
+                                 const float2*, int, const Cand*, const int*, int*,
+                                 unsigned long long*);
+
+// Instantiates the kernels for bands LO..HI into the dispatch tables.
+template <int LO, int HI>
+struct RegRange {
+    static void fill(RegKernel* eu, RegKernel* mh, RegSearchKernel* seu, RegSearchKernel* smh) {
+        if constexpr (LO <= HI) {
+            eu[LO] = cdtw_reg_kernel<LO, true>;
+            mh[LO] = cdtw_reg_kernel<LO, false>;
+            seu[LO] = cdtw_reg_search_kernel<LO, true>;
+            smh[LO] = cdtw_reg_search_kernel<LO, false>;
+            RegRange<LO + 1, HI>::fill(eu, mh, seu, smh);
+        }
+    }
+};
+
+}  // namespace
+
+// Defined in cdtw_reg_part*.cu: each fills its range of bands.
+void reg_fill_part0(void** eu, void** mh, void** seu, void** smh);
+void reg_fill_part1(void** eu, void** mh, void** seu, void** smh);
+void reg_fill_part2(void** eu, void** mh, void** seu, void** smh);
+void reg_fill_part3(void** eu, void** mh, void** seu, void** smh);
+void reg_fill_part4(void** eu, void** mh, void** seu, void** smh);
+void reg_fill_part5(void** eu, void** mh, void** seu, void** smh);
+
+}  // namespace cdtw

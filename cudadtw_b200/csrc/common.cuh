@@ -59,6 +59,9 @@ struct cdtw_handle_s {
     // grow-only device workspace
     void* ws = nullptr;
     size_t ws_bytes = 0;
+    // boundary rings of the strip kernel's resident warps (grow-only)
+    void* ring = nullptr;
+    size_t ring_bytes = 0;
     // query pack storage (grow-only)
     void* qmem = nullptr;
     size_t qmem_bytes = 0;
@@ -68,6 +71,8 @@ struct cdtw_handle_s {
     void* pinned = nullptr;
     // stage counts of the last search: windows, after LB_Kim, after LB_Keogh
     int64_t last_counts[4] = {0, 0, 0, 0};
+    // cDTW kernel variant per band (0 = built-in rule); set by the autotuner
+    unsigned char band_variant[CDTW_MAX_QUERY] = {0};
     char err[512] = {0};
 };
 
@@ -189,6 +194,10 @@ int launch_cdtw_strip(cdtw_handle h, const float* x, int64_t N, const double* mu
                       const float* sigma, const int32_t* idx, int64_t L, bool euclid, int R,
                       float* out);
 int strip_rows_default(int W);
+// Kernel choice for band W: CDTW_VARIANT_REGISTER (one thread per window, band
+// in registers, W <= 96), CDTW_VARIANT_STRIP16 / STRIP32 (strips of 16 / 32
+// rows, W >= 15 / 31).
+int choose_variant(cdtw_handle h, int W);
 int max_register_band();
 int launch_lb_kim(cdtw_handle h, const float* x, int64_t N, const double* mu, const float* sigma,
                   const int32_t* idx, int64_t L, bool euclid, float* out,

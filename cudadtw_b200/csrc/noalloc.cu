@@ -21,12 +21,9 @@
 
 #include <mutex>
 
-namespace cdtw {
-// defined in cdtw_reg.cu
-int max_register_band();
-}
-
 namespace {
+
+constexpr int kNoAllocMaxBand = 40;  // bands served by this entry point
 
 constexpr size_t align256(size_t b) { return (b + 255) / 256 * 256; }
 
@@ -91,9 +88,9 @@ extern "C" int cdtw_all_windows_noalloc(const float* d_query, int M, const float
         return fail(errbuf, errlen, CDTW_EUNSUPPORTED, msg);
     }
     if (W > M - 1) W = M - 1;
-    if (W > max_register_band()) {
+    if (W > kNoAllocMaxBand) {
         snprintf(msg, sizeof(msg), "band %d exceeds the limit %d of this entry point", W,
-                 max_register_band());
+                 kNoAllocMaxBand);
         return fail(errbuf, errlen, CDTW_EUNSUPPORTED, msg);
     }
     int dev = 0;

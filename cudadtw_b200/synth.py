@@ -71,3 +71,23 @@ def band_from_percent(m: int, p: int) -> int:
 def widen(x: np.ndarray) -> np.ndarray:
     """Exact FP64 twin of a float32 array (for the FP64 UCR Suite tools)."""
     return x.astype(np.float64)
+
+
+def batch_queries(stream: np.ndarray, n: int = 512, seed: int = 2, m_lo: int = 64,
+                  m_hi: int = 1024, pcts=(5, 10, 20), noise: float = 0.05):
+    """The batched-search workload: n queries with lengths uniform in
+    [m_lo, m_hi] and band ratios drawn from ``pcts``; the first half cut from
+    ``stream`` at seeded offsets (+ N(0, noise)), the second half independent
+    random walks.  Returns a list of (query float32, W, P, cut offset or -1)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(n):
+        m = int(rng.integers(m_lo, m_hi + 1))
+        p = int(pcts[int(rng.integers(0, len(pcts)))])
+        w = band_from_percent(m, p)
+        if k < n // 2:
+            q, off = cut_query(stream, m, seed=int(rng.integers(1 << 30)), noise=noise)
+        else:
+            q, off = random_walk(m, seed=int(rng.integers(1 << 30))), -1
+        out.append((q, w, p, off))
+    return out

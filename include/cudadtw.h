@@ -205,6 +205,22 @@ int cdtw_all_windows_noalloc(const float* d_query, int M, const float* d_subject
                              int W, int metric, float* d_out, void* cuda_stream,
                              char* errbuf, int errlen);
 
+/* ---- kernel selection ----------------------------------------------------------- */
+
+enum cdtw_variant {
+    CDTW_VARIANT_AUTO = 0,      /* built-in rule: register band for W <= 96, else 16-row strips */
+    CDTW_VARIANT_REGISTER = 1,  /* one thread per window, the band in registers (W <= 96) */
+    CDTW_VARIANT_STRIP16 = 2,   /* strips of 16 rows, boundary ring (W >= 15)            */
+    CDTW_VARIANT_STRIP32 = 3    /* strips of 32 rows, boundary ring (W >= 31)            */
+};
+
+/* Kernel variant for bands w_lo..w_hi on this handle (what the autotuner,
+ * cudadtw_b200/autotune.py, sets per (length, band) bucket).  A variant that
+ * cannot run a band falls back to the built-in rule.  No reference
+ * counterpart (gpu_cdtw's blockdtw flag chooses block vs thread kernels,
+ * include/cdtw.cuh:450-487). */
+int cdtw_set_band_variant(cdtw_handle h, int w_lo, int w_hi, int variant);
+
 /* ---- measurement ------------------------------------------------------------ */
 
 /* Issue-bound peak cell-update rate of the device (cells/s): the minimal cell
