@@ -35,6 +35,8 @@ SIGNATURES = {
     "cdtw_search_host": (c_int, [c_vp, c_vp, c_int, c_vp, c_i64, c_int, c_int, c_i64p, c_f32p]),
     "cdtw_search_counts": (c_int, [c_vp, c_i64p]),
     "cdtw_set_band_variant": (c_int, [c_vp, c_int, c_int, c_int]),
+    "cdtw_search_batched": (c_int, [c_vp, c_vp, c_i64, c_vp, c_vp, c_vp, c_int, c_int, c_vp, c_vp,
+                                    c_vp, c_vp]),
     "ed_all_windows": (c_int, [c_vp, c_vp, c_int, c_vp, c_i64, c_vp]),
     "ed_search_host": (c_int, [c_vp, c_vp, c_int, c_vp, c_i64, c_i64p, c_f64p]),
     "ldtw_all_windows": (c_int, [c_vp, c_vp, c_i64, c_int, c_vp]),

@@ -251,3 +251,25 @@ class Handle:
         """cDTW kernel variant for bands w_lo..w_hi (the autotuner's knob)."""
         v = self.VARIANTS[variant] if isinstance(variant, str) else int(variant)
         self._check(self._lib.cdtw_set_band_variant(self._h, w_lo, w_hi, v))
+
+    # -- batched search ---------------------------------------------------------
+    def search_batched(self, subject: torch.Tensor, queries, bands, metric=EUCLIDEAN,
+                       rows=None, tiles=None):
+        """Best match (locations, distances) of every query in one graph launch
+        of the persistent batched search.  ``queries``: list of 1-D arrays,
+        ``bands``: W per query; ``rows`` / ``tiles``: per-query tile shape
+        (None = built-in rule; the autotuner fills them per bucket)."""
+        _dev(subject, torch.float32, "subject")
+        qs = [np.ascontiguousarray(q, dtype=np.float32) for q in queries]
+        nq = len(qs)
+        flat = np.concatenate(qs) if nq else np.zeros(0, np.float32)
+        ms = np.array([q.size for q in qs], dtype=np.int32)
+        ws = np.ascontiguousarray(bands, dtype=np.int32)
+        r = None if rows is None else np.ascontiguousarray(rows, dtype=np.int32)
+        t = None if tiles is None else np.ascontiguousarray(tiles, dtype=np.int32)
+        locs = np.empty(nq, np.int64)
+        dists = np.empty(nq, np.float32)
+        self._check(self._lib.cdtw_search_batched(
+            self._h, _ptr(subject), subject.numel(), _ptr(flat), _ptr(ms), _ptr(ws), nq,
+            _metric(metric), _ptr(r), _ptr(t), _ptr(locs), _ptr(dists)))
+        return locs, dists

@@ -22,53 +22,17 @@ namespace cdtw {
 namespace {
 
 template <bool EU>
-__device__ __forceinline__ float lp(float d) { return EU ? d * d : fabsf(d); }
-
-// 5x5 unconstrained DTW at the front (min over last row and column) plus the
-// 5x5 block at the back entered from anywhere on its first row/column,
-// exactly the recurrences of bounds.cuh:315-404.
-template <bool EU>
 __device__ __forceinline__ float lb_kim_window(const float* __restrict__ xw, const Norm& nm,
                                                const float* __restrict__ zq, int M) {
-    float s[5], q[5], F[5], G[5];
+    float sv[10], qv[10];
 #pragma unroll
     for (int k = 0; k < 5; ++k) {
-        s[k] = znorm(nm, __ldg(xw + k));
-        q[k] = __ldg(zq + k);
+        sv[k] = znorm(nm, __ldg(xw + k));
+        qv[k] = __ldg(zq + k);
+        sv[5 + k] = znorm(nm, __ldg(xw + M - 5 + k));
+        qv[5 + k] = __ldg(zq + M - 5 + k);
     }
-    // front: rows = query 0..4, cols = window 0..4
-    F[0] = lp<EU>(q[0] - s[0]);
-#pragma unroll
-    for (int k = 1; k < 5; ++k) F[k] = lp<EU>(q[0] - s[k]) + F[k - 1];
-    float mem = F[4];
-#pragma unroll
-    for (int r = 1; r < 5; ++r) {
-        G[0] = lp<EU>(q[r] - s[0]) + F[0];
-#pragma unroll
-        for (int k = 1; k < 5; ++k) G[k] = lp<EU>(q[r] - s[k]) + min3f(G[k - 1], F[k - 1], F[k]);
-        mem = fminf(mem, G[4]);
-#pragma unroll
-        for (int k = 0; k < 5; ++k) F[k] = G[k];
-    }
-#pragma unroll
-    for (int k = 0; k < 4; ++k) mem = fminf(mem, F[k]);
-    // back: the path may enter anywhere on the block's first row / column
-#pragma unroll
-    for (int k = 0; k < 5; ++k) {
-        s[k] = znorm(nm, __ldg(xw + M - 5 + k));
-        q[k] = __ldg(zq + M - 5 + k);
-    }
-#pragma unroll
-    for (int k = 0; k < 5; ++k) F[k] = lp<EU>(q[0] - s[k]);
-#pragma unroll
-    for (int r = 1; r < 5; ++r) {
-        G[0] = lp<EU>(q[r] - s[0]);
-#pragma unroll
-        for (int k = 1; k < 5; ++k) G[k] = lp<EU>(q[r] - s[k]) + min3f(G[k - 1], F[k - 1], F[k]);
-#pragma unroll
-        for (int k = 0; k < 5; ++k) F[k] = G[k];
-    }
-    return mem + F[4];
+    return lb_kim_dp<EU>(sv, qv);
 }
 
 template <bool EU>

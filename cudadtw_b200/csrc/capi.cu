@@ -151,6 +151,8 @@ int cdtw_destroy(cdtw_handle h) {
     if (!h) return CDTW_EINVAL;
     cudaSetDevice(h->device);
     cudaStreamSynchronize(h->stream);
+    if (h->own_stream) cudaStreamSynchronize(h->own_stream);
+    batch_plan_release(h);
     if (h->ws) cudaFree(h->ws);
     if (h->qmem) cudaFree(h->qmem);
     if (h->ring) cudaFree(h->ring);

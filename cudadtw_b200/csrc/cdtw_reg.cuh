@@ -86,13 +86,73 @@ cdtw_reg_kernel(const float* __restrict__ x, const double* __restrict__ mu,
     out[t] = res;
 }
 
+// cDTW of one window (xw, normalisation nm) against the query whose padded
+// copies sit in shared memory (sq4, lq4 float4 per copy) with its envelope
+// senv, abandoning once the last row minimum plus the remaining suffix of the
+// window's forward LB_Keogh lbk (the cumulative bound cb of
+// UCR_DTW_BIN.cpp:666-677, :336) reaches the best-so-far in *key.  alive
+// marks lanes still worth finishing; the warp stops when no lane is.  All 32
+// lanes call together.  Returns +inf if the warp stopped early.
+template <int W, bool EU>
+__device__ __forceinline__ float reg_window_dtw(const float4* sq4, int lq4,
+                                                const float2* senv, int M,
+                                                const float* __restrict__ xw, const Norm& nm,
+                                                float lbk, bool& alive,
+                                                const unsigned long long* key) {
+    constexpr int B = 2 * W + 1;
+    constexpr int NQ4 = (B + 3) / 4;
+    float prev[B + 1];
+#pragma unroll
+    for (int k = 0; k <= B; ++k) prev[k] = CDTW_INF;
+    prev[W] = 0.0f;
+    float res = CDTW_INF, pre = 0.f;
+    for (int j0 = 0; j0 < M; j0 += 4) {
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int j = j0 + u;
+            const int jc = min(j, M - 1);
+            const float z = znorm(nm, __ldg(xw + jc));
+            // forward LB_Keogh term of this data row (query envelope at j)
+            const float2 e = senv[jc];
+            const float dl = max3f(z - e.y, e.x - z, 0.f);
+            pre += (j < M) ? (EU ? dl * dl : dl) : 0.f;
+            const float4* qr = sq4 + u * lq4 + (j0 >> 2);
+            float qv[NQ4 * 4];
+#pragma unroll
+            for (int r = 0; r < NQ4; ++r) {
+                const float4 v = qr[r];
+                qv[4 * r + 0] = v.x;
+                qv[4 * r + 1] = v.y;
+                qv[4 * r + 2] = v.z;
+                qv[4 * r + 3] = v.w;
+            }
+            float left = CDTW_INF;
+            float cur[B];
+#pragma unroll
+            for (int k = 0; k < B; ++k) {
+                const float m = min3f(prev[k], prev[k + 1], left);
+                left = cell<EU>(z - qv[k], m);
+                cur[k] = left;
+            }
+            if (j == M - 1) res = cur[W];
+#pragma unroll
+            for (int k = 0; k < B; ++k) prev[k] = cur[k];
+        }
+        if ((j0 & 7) == 4 && j0 + 3 < M - 1) {  // rows j0..j0+3 are all real rows
+            float rmin = prev[0];
+#pragma unroll
+            for (int k = 1; k < B; k += 2) rmin = min3f(rmin, prev[k], prev[k + 1]);
+            alive = alive && (rmin + (lbk - pre) * kLbSlack < load_bsf(key));
+            if (!__any_sync(0xffffffffu, alive)) return CDTW_INF;
+        }
+    }
+    return res;
+}
+
 // Search variant: persistent warps take 32 candidates at a time from a device
 // list, skip those whose lower bound already exceeds the best-so-far, run the
-// register-band DTW, and abandon a candidate once its last row minimum plus
-// the remaining suffix of its forward LB_Keogh (the cumulative bound cb of
-// UCR_DTW_BIN.cpp:666-677, :336) reaches the best-so-far.  The warp leaves a
-// group when all 32 lanes have abandoned.  Results fold into *key by a packed
-// (distance, window) atomicMin, so ties keep the lowest window.
+// register-band DTW with early abandoning, and fold results into *key by a
+// packed (distance, window) atomicMin, so ties keep the lowest window.
 template <int W, bool EU>
 __global__ void __launch_bounds__(kRegBlock)
 cdtw_reg_search_kernel(const float* __restrict__ x, const double* __restrict__ mu,
@@ -107,8 +167,6 @@ cdtw_reg_search_kernel(const float* __restrict__ x, const double* __restrict__ m
     __syncthreads();
     const int lane = threadIdx.x & 31;
     const int n = *(const volatile int*)count;
-    constexpr int B = 2 * W + 1;
-    constexpr int NQ4 = (B + 3) / 4;
     for (;;) {
         int base = 0;
         if (lane == 0) base = atomicAdd(work, 32);
@@ -120,59 +178,11 @@ cdtw_reg_search_kernel(const float* __restrict__ x, const double* __restrict__ m
         c.lb = CDTW_INF;
         c.lbk = 0.f;
         if (i < n) c = cands[i];
-        float bsf = load_bsf(key);
-        bool alive = (i < n) && (c.lb * kLbSlack < bsf);
+        bool alive = (i < n) && (c.lb * kLbSlack < load_bsf(key));
         if (!__any_sync(0xffffffffu, alive)) continue;
-        const int w = c.w;
-        const Norm nm = make_norm(mu[w], sigma[w]);
-        const float* __restrict__ xw = x + w;
-        float prev[B + 1];
-#pragma unroll
-        for (int k = 0; k <= B; ++k) prev[k] = CDTW_INF;
-        prev[W] = 0.0f;
-        float res = CDTW_INF, pre = 0.f;
-        for (int j0 = 0; j0 < M; j0 += 4) {
-#pragma unroll
-            for (int u = 0; u < 4; ++u) {
-                const int j = j0 + u;
-                const int jc = min(j, M - 1);
-                const float z = znorm(nm, __ldg(xw + jc));
-                // forward LB_Keogh term of this data row (query envelope at j)
-                const float2 e = senv[jc];
-                const float dl = max3f(z - e.y, e.x - z, 0.f);
-                pre += (j < M) ? (EU ? dl * dl : dl) : 0.f;
-                const float4* qr = sq4 + u * lq4 + (j0 >> 2);
-                float qv[NQ4 * 4];
-#pragma unroll
-                for (int r = 0; r < NQ4; ++r) {
-                    const float4 v = qr[r];
-                    qv[4 * r + 0] = v.x;
-                    qv[4 * r + 1] = v.y;
-                    qv[4 * r + 2] = v.z;
-                    qv[4 * r + 3] = v.w;
-                }
-                float left = CDTW_INF;
-                float cur[B];
-#pragma unroll
-                for (int k = 0; k < B; ++k) {
-                    const float m = min3f(prev[k], prev[k + 1], left);
-                    left = cell<EU>(z - qv[k], m);
-                    cur[k] = left;
-                }
-                if (j == M - 1) res = cur[W];
-#pragma unroll
-                for (int k = 0; k < B; ++k) prev[k] = cur[k];
-            }
-            if ((j0 & 7) == 4 && j0 + 3 < M - 1) {  // rows j0..j0+3 are all real rows
-                float rmin = prev[0];
-#pragma unroll
-                for (int k = 1; k < B; k += 2) rmin = min3f(rmin, prev[k], prev[k + 1]);
-                bsf = load_bsf(key);
-                alive = alive && (rmin + (c.lbk - pre) * kLbSlack < bsf);
-                if (!__any_sync(0xffffffffu, alive)) break;
-            }
-        }
-        if (i < n && res < CDTW_INF) atomicMin(key, pack_key(res, (uint32_t)w));
+        const Norm nm = make_norm(mu[c.w], sigma[c.w]);
+        const float res = reg_window_dtw<W, EU>(sq4, lq4, senv, M, x + c.w, nm, c.lbk, alive, key);
+        if (i < n && res < CDTW_INF) atomicMin(key, pack_key(res, (uint32_t)c.w));
     }
 }
 

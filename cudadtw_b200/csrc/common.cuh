@@ -59,6 +59,8 @@ struct cdtw_handle_s {
     // grow-only device workspace
     void* ws = nullptr;
     size_t ws_bytes = 0;
+    // cached plan of the batched search (batch_host.cu)
+    void* batch = nullptr;
     // boundary rings of the strip kernel's resident warps (grow-only)
     void* ring = nullptr;
     size_t ring_bytes = 0;
@@ -79,6 +81,7 @@ struct cdtw_handle_s {
 namespace cdtw {
 
 int set_error(cdtw_handle h, int status, const char* fmt, ...);
+void batch_plan_release(cdtw_handle h);
 int check_cuda(cdtw_handle h, cudaError_t e, const char* what);
 int ensure_workspace(cdtw_handle h, size_t bytes);
 
@@ -132,6 +135,44 @@ __device__ __forceinline__ float znorm(const Norm& n, float x) {
     return fmaf(x - n.mhi, n.s, n.c);
 }
 
+// LB_Kim of the reference GPU path on ten z-normalised window samples
+// s[0..4] (front) / s[5..9] (back) and the matching query values q[0..9]:
+// 5x5 unconstrained DTW at the front (min over its last row and column) plus
+// the 5x5 back block entered anywhere on its first row/column, the
+// recurrences of include/bounds.cuh:315-404.
+template <bool EU>
+__device__ __forceinline__ float lb_kim_dp(const float (&s)[10], const float (&q)[10]) {
+    auto lp = [](float d) { return EU ? d * d : fabsf(d); };
+    float F[5], G[5];
+    F[0] = lp(q[0] - s[0]);
+#pragma unroll
+    for (int k = 1; k < 5; ++k) F[k] = lp(q[0] - s[k]) + F[k - 1];
+    float mem = F[4];
+#pragma unroll
+    for (int r = 1; r < 5; ++r) {
+        G[0] = lp(q[r] - s[0]) + F[0];
+#pragma unroll
+        for (int k = 1; k < 5; ++k) G[k] = lp(q[r] - s[k]) + min3f(G[k - 1], F[k - 1], F[k]);
+        mem = fminf(mem, G[4]);
+#pragma unroll
+        for (int k = 0; k < 5; ++k) F[k] = G[k];
+    }
+#pragma unroll
+    for (int k = 0; k < 4; ++k) mem = fminf(mem, F[k]);
+#pragma unroll
+    for (int k = 0; k < 5; ++k) F[k] = lp(q[5] - s[5 + k]);
+#pragma unroll
+    for (int r = 1; r < 5; ++r) {
+        G[0] = lp(q[5 + r] - s[5]);
+#pragma unroll
+        for (int k = 1; k < 5; ++k)
+            G[k] = lp(q[5 + r] - s[5 + k]) + min3f(G[k - 1], F[k - 1], F[k]);
+#pragma unroll
+        for (int k = 0; k < 5; ++k) F[k] = G[k];
+    }
+    return mem + F[4];
+}
+
 // Packed (distance, index) key for the fused argmin: distances are >= 0 so
 // their float bits order like unsigned ints; ties keep the lowest index
 // (UCR's first strict minimum, UCR_DTW_BIN.cpp:682).
@@ -152,6 +193,16 @@ struct Cand {
     float lb;
     float lbk;
 };
+
+// Number of seed windows whose cDTW gives a query its first best-so-far:
+// about kSeedCells band cells in total (a few tens of microseconds of cDTW),
+// at least 64 and at most 4096 windows.
+constexpr double kSeedCells = 2.0e8;
+__host__ __device__ inline int seed_target(int M, int W) {
+    const double cells = (double)M * (2.0 * W + 1.0) - (double)W * (W + 1.0);
+    const double n = kSeedCells / (cells > 1.0 ? cells : 1.0);
+    return n < 64.0 ? 64 : (n > 4096.0 ? 4096 : (int)n);
+}
 
 // Lower bounds are compared against the best-so-far with this relative
 // slack, so FP32 rounding of a bound can never prune a window whose distance
@@ -187,6 +238,9 @@ int launch_ed(cdtw_handle h, const double* x, int64_t N, const double* zq, int M
 int launch_ldtw(cdtw_handle h, const float* x, int64_t N, const double* mu, const double* sigma,
                 bool euclid, double* out);
 int launch_prepare_query(cdtw_handle h, const float* d_query_raw, int M, int W);
+// One block per query: prepares packs[q] from the raw query at raw + offs[q].
+int launch_prepare_queries(cdtw_handle h, const float* raw, const int64_t* offs,
+                           const QueryPack* packs, int nq, int max_m);
 int launch_cdtw_windows(cdtw_handle h, const float* x, int64_t N, const double* mu,
                         const float* sigma, const int32_t* idx, int64_t L, bool euclid,
                         float* out);

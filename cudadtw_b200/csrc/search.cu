@@ -41,7 +41,6 @@ struct SearchWs {
 };
 
 constexpr int kKimBlock = 256;
-constexpr int kMaxSeeds = 4096;  // seed windows whose cDTW gives the first best-so-far
 
 // Seed candidates: the smallest LB_Kim window of each group of G blocks.
 __global__ void seeds_to_cands_kernel(const unsigned long long* __restrict__ seeds, int nblk,
@@ -172,7 +171,7 @@ int run_search(cdtw_handle h, const float* x, int64_t N, const double* mu, const
     const int64_t nblk = div_up(Nw, kKimBlock);
     CDTW_TRY(launch_lb_kim(h, x, N, mu, sigma, nullptr, Nw, euclid, ws.lbkim, ws.seeds));
     // 2. cDTW of the seeds
-    const int G = (int)std::max<int64_t>(1, div_up(nblk, kMaxSeeds));
+    const int G = (int)std::max<int64_t>(1, div_up(nblk, seed_target(q.M, q.W)));
     const int nseed = (int)div_up(nblk, G);
     seeds_to_cands_kernel<<<(unsigned)div_up(nseed, 256), 256, 0, h->stream>>>(
         ws.seeds, (int)nblk, G, ws.seed_cands, ws.ctr + 4);

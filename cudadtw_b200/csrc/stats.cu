@@ -81,10 +81,9 @@ avg_std_kernel(const XT* __restrict__ x, int64_t N, int M, double* __restrict__ 
 // reference does this on the host in FP32, GPU-dtw.cu:67 / stats.cuh:8-28),
 // the +inf-padded shifted copies read by the cDTW kernels, and the +-W
 // envelope (same values as Lemire's filter, bounds.cuh:13-64).
-__global__ void __launch_bounds__(256)
-prepare_query_kernel(const float* __restrict__ qraw, int M, int W, QueryPack p) {
+__device__ __forceinline__ void prepare_query_body(const float* __restrict__ qraw, int M, int W,
+                                                   const QueryPack& p, double* zs) {
     __shared__ double red[2][8];
-    extern __shared__ double zs[];  // M doubles
     const int t = threadIdx.x, lane = t & 31, wid = t >> 5;
     double s = 0.0;
     for (int i = t; i < M; i += blockDim.x) {
@@ -119,7 +118,7 @@ prepare_query_kernel(const float* __restrict__ qraw, int M, int W, QueryPack p) 
     }
     __syncthreads();
     // padded shifted copies: copy m, index a -> qp[a+m], qp[b] = zq[b-W]
-    for (int e = t; e < 4 * p.lq; e += blockDim.x) {
+    for (int e = t; p.qpad && e < 4 * p.lq; e += blockDim.x) {
         const int m = e / p.lq, a = e - m * p.lq;
         const int i = a + m - W;
         p.qpad[e] = (i >= 0 && i < M) ? (float)zs[i] : CDTW_INF;
@@ -149,6 +148,20 @@ prepare_query_kernel(const float* __restrict__ qraw, int M, int W, QueryPack p) 
     }
 }
 
+__global__ void __launch_bounds__(256)
+prepare_query_kernel(const float* __restrict__ qraw, int M, int W, QueryPack p) {
+    extern __shared__ double zs[];  // M doubles
+    prepare_query_body(qraw, M, W, p, zs);
+}
+
+__global__ void __launch_bounds__(256)
+prepare_queries_kernel(const float* __restrict__ raw, const int64_t* __restrict__ offs,
+                       const QueryPack* __restrict__ packs) {
+    extern __shared__ double zs[];
+    const QueryPack p = packs[blockIdx.x];
+    prepare_query_body(raw + offs[blockIdx.x], p.M, p.W, p, zs);
+}
+
 }  // namespace
 
 int launch_avg_std(cdtw_handle h, const float* x, int64_t N, int M, double* mu, float* sigma) {
@@ -174,6 +187,18 @@ int launch_avg_std64(cdtw_handle h, const double* x, int64_t N, int M, double* m
     avg_std_kernel<double, double><<<(unsigned)blocks, kStatsBlock, 0, h->stream>>>(x, N, M, mu,
                                                                                     sigma);
     CDTW_LAUNCH(h, "avg_std_kernel");
+    return CDTW_OK;
+}
+
+int launch_prepare_queries(cdtw_handle h, const float* raw, const int64_t* offs,
+                           const QueryPack* packs, int nq, int max_m) {
+    const size_t smem = (size_t)max_m * sizeof(double);
+    if (smem > 48 * 1024)
+        CDTW_CUDA(h, cudaFuncSetAttribute((const void*)prepare_queries_kernel,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)smem));
+    prepare_queries_kernel<<<nq, 256, smem, h->stream>>>(raw, offs, packs);
+    CDTW_LAUNCH(h, "prepare_queries_kernel");
     return CDTW_OK;
 }
 

@@ -140,6 +140,27 @@ int cdtw_search_host(cdtw_handle h, const float* h_query, int M, const float* h_
  * pruning percentages, UCR_DTW_BIN.cpp:738-741). */
 int cdtw_search_counts(cdtw_handle h, int64_t* counts);
 
+/* ---- batched search ------------------------------------------------------------- */
+
+/* Best match of each of nq queries (lengths Ms[q] in [11, 4096], bands Ws[q];
+ * the raw float32 values concatenated in h_queries) in one device subject.
+ * No reference counterpart: the reference searches one query per process.
+ * The whole batch runs as one CUDA graph of persistent kernels that pull
+ * (query, stream-tile) work items from device queues: a seed pass (window
+ * statistics + LB_Kim per tile), the cDTW of the seed windows, and a main
+ * pass (statistics, LB_Kim, LB_Keogh, early-abandoning strip cDTW of the
+ * survivors).  rows[q] chooses the main-pass cDTW of the query's (length,
+ * band) bucket: 0 = register band (one kernel per W <= 96), 1/2/4/8/16 =
+ * strips of that many rows (W >= rows-1); tiles[q] is the windows per work
+ * item (a multiple of 32 in [32, 4096]).  NULL selects the built-in rule
+ * (register band up to W = 96, 16-row strips above, 1024-window tiles).  The graph is built on the first call and replayed while the subject
+ * pointer, N, lengths, bands, shapes and metric stay the same.  Results as
+ * cdtw_prune_cdtw: window start (lowest on ties) and printed distance. */
+int cdtw_search_batched(cdtw_handle h, const float* d_subject, int64_t N,
+                        const float* h_queries, const int* Ms, const int* Ws, int nq,
+                        int metric, const int* rows, const int* tiles, int64_t* locations,
+                        float* distances);
+
 /* ---- GPU-ED: z-normalised Euclidean distance (float64) --------------------------- */
 
 /* Squared z-normalised Euclidean distance of the query to every window,
