@@ -43,6 +43,10 @@ SIGNATURES = {
     "ldtw_search_host": (c_int, [c_vp, c_vp, c_int, c_vp, c_i64, c_int, c_int, c_i64p, c_f64p]),
     "cdtw_all_windows_noalloc": (c_int, [c_vp, c_int, c_vp, c_i64, c_int, c_int, c_vp, c_vp,
                                          ctypes.c_char_p, c_int]),
+    "cdtw_pair_path_bytes": (ctypes.c_size_t, [c_i64, c_int]),
+    "cdtw_pair_fwd": (c_int, [c_vp, c_vp, c_vp, c_i64, c_int, c_int, c_int, c_int, c_vp, c_vp]),
+    "cdtw_pair_bwd": (c_int, [c_vp, c_vp, c_vp, c_i64, c_int, c_int, c_int, c_vp, c_vp, c_vp,
+                              c_vp]),
 }
 
 _lib = None
@@ -74,4 +78,4 @@ def declared_symbols() -> list[str]:
     """Every function declared in include/cudadtw.h (parsed from the header)."""
     import re
     text = open(HEADER).read()
-    return sorted(set(re.findall(r"^\s*(?:int|const char\*|void)\s+(\w+)\s*\(", text, re.M)))
+    return sorted(set(re.findall(r"^\s*(?:int|const char\*|void|size_t)\s+(\w+)\s*\(", text, re.M)))

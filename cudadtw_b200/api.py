@@ -273,3 +273,42 @@ class Handle:
             self._h, _ptr(subject), subject.numel(), _ptr(flat), _ptr(ms), _ptr(ws), nq,
             _metric(metric), _ptr(r), _ptr(t), _ptr(locs), _ptr(dists)))
         return locs, dists
+
+    # -- differentiable pairwise cDTW -------------------------------------------
+    PAIR_ZNORM = 1
+
+    def pair_path_bytes(self, n: int, L: int) -> int:
+        """Bytes of the path record cdtw_pair_fwd writes for n pairs of length L."""
+        return int(self._lib.cdtw_pair_path_bytes(n, L))
+
+    def pair_fwd(self, q: torch.Tensor, s: torch.Tensor, W: int, metric=EUCLIDEAN,
+                 znorm: bool = True, path: torch.Tensor | None = None,
+                 out: torch.Tensor | None = None) -> torch.Tensor:
+        """Banded cDTW of every pair (q[p], s[p]) (device (n, L) float32).  With
+        ``path`` (a uint8 device buffer of pair_path_bytes) the optimal path is
+        recorded for pair_bwd."""
+        _dev(q, torch.float32, "q")
+        _dev(s, torch.float32, "s")
+        if q.shape != s.shape or q.dim() != 2:
+            raise ValueError("q and s must both be (n, L)")
+        n, L = q.shape
+        D = out if out is not None else torch.empty(n, dtype=torch.float32, device=q.device)
+        self._check(self._lib.cdtw_pair_fwd(self._h, _ptr(q), _ptr(s), n, L, int(W),
+                                            _metric(metric), self.PAIR_ZNORM if znorm else 0,
+                                            _ptr(D), _ptr(path)))
+        return D
+
+    def pair_bwd(self, q: torch.Tensor, s: torch.Tensor, path: torch.Tensor, dD=None,
+                 metric=EUCLIDEAN, znorm: bool = True, need_q: bool = True,
+                 need_s: bool = True, dq: torch.Tensor | None = None,
+                 ds: torch.Tensor | None = None):
+        """Gradients (dq, ds) of sum_p dD[p] * D[p] along the recorded paths."""
+        n, L = q.shape
+        if need_q and dq is None:
+            dq = torch.empty_like(q)
+        if need_s and ds is None:
+            ds = torch.empty_like(s)
+        self._check(self._lib.cdtw_pair_bwd(
+            self._h, _ptr(q), _ptr(s), n, L, _metric(metric), self.PAIR_ZNORM if znorm else 0,
+            _ptr(path), _ptr(dD), _ptr(dq if need_q else None), _ptr(ds if need_s else None)))
+        return (dq if need_q else None), (ds if need_s else None)

@@ -487,6 +487,69 @@ int ldtw_search_host(cdtw_handle h, const float* h_query, int M, const float* h_
     return CDTW_OK;
 }
 
+size_t cdtw_pair_path_bytes(int64_t n, int L) {
+    if (n <= 0 || L <= 0) return 0;
+    return (size_t)n * 32 + (size_t)n * L * 8;
+}
+
+static int pair_check(cdtw_handle h, const float* q, const float* s, int64_t n, int L,
+                      int metric, int flags) {
+    if (!q || !s || n < 0 || L < 1 || L > CDTW_MAX_QUERY)
+        return set_error(h, CDTW_EINVAL, "bad pair arguments (n=%lld L=%d)", (long long)n, L);
+    if (!valid_metric(metric)) return set_error(h, CDTW_EINVAL, "bad metric %d", metric);
+    if (flags & ~CDTW_PAIR_ZNORM) return set_error(h, CDTW_EINVAL, "bad flags %d", flags);
+    if (n > (int64_t)INT32_MAX * 4) return set_error(h, CDTW_EINVAL, "too many pairs");
+    return CDTW_OK;
+}
+
+int cdtw_pair_fwd(cdtw_handle h, const float* d_q, const float* d_s, int64_t n, int L, int W,
+                  int metric, int flags, float* d_D, void* d_path) {
+    if (!h) return CDTW_EINVAL;
+    CDTW_TRY(pair_check(h, d_q, d_s, n, L, metric, flags));
+    if (!d_D || W < 0) return set_error(h, CDTW_EINVAL, "bad output or band");
+    if (n == 0) return CDTW_OK;
+    W = std::min(W, L - 1);
+    if (W > CDTW_PAIR_MAX_BAND)
+        return set_error(h, CDTW_EUNSUPPORTED, "pair band W=%d exceeds %d", W, CDTW_PAIR_MAX_BAND);
+    if (d_path && ((uintptr_t)d_path & 7))
+        return set_error(h, CDTW_EINVAL, "path record must be 8-byte aligned");
+    const bool zn = flags & CDTW_PAIR_ZNORM;
+    Carver c;
+    const size_t o_zq = zn ? c.take<float>((size_t)n * L) : 0;
+    const size_t o_zs = zn ? c.take<float>((size_t)n * L) : 0;
+    const size_t o_dirs = d_path ? c.take<uint32_t>((size_t)n * pair_dirs_words(L, W)) : 0;
+    CDTW_TRY(ensure_workspace(h, c.off));
+    char* ws = (char*)h->ws;
+    double* hdr = (double*)d_path;
+    uint32_t* rows = d_path ? (uint32_t*)((char*)d_path + (size_t)n * 32) : nullptr;
+    uint32_t* cols = d_path ? rows + (size_t)n * L : nullptr;
+    const float* zq = d_q;
+    const float* zs = d_s;
+    if (zn) {
+        CDTW_TRY(launch_pair_znorm(h, d_q, d_s, n, L, (float*)(ws + o_zq), (float*)(ws + o_zs),
+                                   hdr));
+        zq = (const float*)(ws + o_zq);
+        zs = (const float*)(ws + o_zs);
+    }
+    return launch_pair_fwd(h, zq, zs, n, L, W, metric == CDTW_EUCLIDEAN, d_D,
+                           d_path ? (uint32_t*)(ws + o_dirs) : nullptr, rows, cols);
+}
+
+int cdtw_pair_bwd(cdtw_handle h, const float* d_q, const float* d_s, int64_t n, int L,
+                  int metric, int flags, const void* d_path, const float* d_dD, float* d_dq,
+                  float* d_ds) {
+    if (!h) return CDTW_EINVAL;
+    CDTW_TRY(pair_check(h, d_q, d_s, n, L, metric, flags));
+    if (!d_path) return set_error(h, CDTW_EINVAL, "no path record");
+    if ((uintptr_t)d_path & 7) return set_error(h, CDTW_EINVAL, "path record must be 8-byte aligned");
+    if (n == 0 || (!d_dq && !d_ds)) return CDTW_OK;
+    const double* hdr = (flags & CDTW_PAIR_ZNORM) ? (const double*)d_path : nullptr;
+    const uint32_t* rows = (const uint32_t*)((const char*)d_path + (size_t)n * 32);
+    const uint32_t* cols = rows + (size_t)n * L;
+    return launch_pair_bwd(h, d_q, d_s, n, L, hdr, rows, cols, d_dD, metric == CDTW_EUCLIDEAN,
+                           d_dq, d_ds);
+}
+
 int cdtw_set_band_variant(cdtw_handle h, int w_lo, int w_hi, int variant) {
     if (!h) return CDTW_EINVAL;
     if (variant < CDTW_VARIANT_AUTO || variant > CDTW_VARIANT_STRIP32 || w_lo < 0 || w_hi < w_lo)

@@ -82,6 +82,16 @@ namespace cdtw {
 
 int set_error(cdtw_handle h, int status, const char* fmt, ...);
 void batch_plan_release(cdtw_handle h);
+// pairwise cDTW forward / backward (pair.cu)
+void pair_shape(int L, int W, int* G, int* C);
+size_t pair_dirs_words(int L, int W);
+int launch_pair_znorm(cdtw_handle h, const float* q, const float* s, int64_t n, int L, float* zq,
+                      float* zs, double* hdr);
+int launch_pair_fwd(cdtw_handle h, const float* zq, const float* zs, int64_t n, int L, int W,
+                    bool euclid, float* D, uint32_t* dirs, uint32_t* rows, uint32_t* cols);
+int launch_pair_bwd(cdtw_handle h, const float* q, const float* s, int64_t n, int L,
+                    const double* hdr, const uint32_t* rows, const uint32_t* cols,
+                    const float* dD, bool euclid, float* dq, float* ds);
 int check_cuda(cdtw_handle h, cudaError_t e, const char* what);
 int ensure_workspace(cdtw_handle h, size_t bytes);
 

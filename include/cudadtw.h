@@ -226,6 +226,37 @@ int cdtw_all_windows_noalloc(const float* d_query, int M, const float* d_subject
                              int W, int metric, float* d_out, void* cuda_stream,
                              char* errbuf, int errlen);
 
+/* ---- differentiable pairwise cDTW --------------------------------------------- */
+
+#define CDTW_PAIR_ZNORM 1      /* z-normalise both series of every pair */
+#define CDTW_PAIR_MAX_BAND 511 /* largest band W (after clamping W to L-1) */
+
+/* Bytes of the path record of n pairs of length L: per pair the
+ * z-normalisation constants (4 doubles) and the warping path as row and
+ * column runs (2 x L 32-bit words).  8-byte aligned device memory. */
+size_t cdtw_pair_path_bytes(int64_t n, int L);
+
+/* Banded cDTW of n pairs (d_q[p], d_s[p]), each L float32 samples, row-major
+ * n x L on the device: d_D[p] = minimum over warping paths with |i-j| <= W of
+ * the summed cell cost (squared difference for CDTW_EUCLIDEAN, absolute for
+ * CDTW_MANHATTAN), the recurrence of include/cdtw.cuh:24-88 on two series.
+ * flags & CDTW_PAIR_ZNORM normalises each series first (population sigma,
+ * sigma = 1 when the variance is 0).  d_path (cdtw_pair_path_bytes, may be
+ * NULL) receives the optimal path for cdtw_pair_bwd; the path is the
+ * minimum-cost one under the rule: diagonal predecessor on ties, then
+ * (i-1, j), then (i, j-1).  No reference counterpart.  1 <= L <= 8192. */
+int cdtw_pair_fwd(cdtw_handle h, const float* d_q, const float* d_s, int64_t n, int L, int W,
+                  int metric, int flags, float* d_D, void* d_path);
+
+/* Gradient of sum_p d_dD[p] * D[p] with respect to the raw inputs (through the
+ * z-normalisation when flags has CDTW_PAIR_ZNORM): the subgradient along the
+ * path recorded by cdtw_pair_fwd, which must have run with the same inputs,
+ * L, metric and flags.  d_dD may be NULL (all ones); d_dq or d_ds may be NULL
+ * to skip that side.  Outputs n x L float32. */
+int cdtw_pair_bwd(cdtw_handle h, const float* d_q, const float* d_s, int64_t n, int L,
+                  int metric, int flags, const void* d_path, const float* d_dD, float* d_dq,
+                  float* d_ds);
+
 /* ---- kernel selection ----------------------------------------------------------- */
 
 enum cdtw_variant {

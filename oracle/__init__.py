@@ -25,6 +25,8 @@ _lib = None
 _f64p = ctypes.POINTER(ctypes.c_double)
 _f32p = ctypes.POINTER(ctypes.c_float)
 _i64p = ctypes.POINTER(ctypes.c_int64)
+_i32p = ctypes.POINTER(ctypes.c_int32)
+_u32p = ctypes.POINTER(ctypes.c_uint32)
 _i64 = ctypes.c_int64
 _int = ctypes.c_int
 
@@ -58,6 +60,12 @@ def lib():
             "orc_ed_all": (None, [_f64p, _int, _f64p, _i64, _f64p]),
             "orc_cdtw_ref_f32": (None, [_f32p, _int, _f32p, _f32p, _f32p, _i64p, _i64, _int,
                                         _int, _f32p]),
+            "orc_pair_fwdbwd": (None, [_f32p, _f32p, _i64, _int, _int, _int, _int, _int, _f32p,
+                                       _f64p, _f64p, _f64p, _f64p]),
+            "orc_pair_fwdbwd64": (None, [_f64p, _f64p, _i64, _int, _int, _int, _int, _f64p, _f64p,
+                                         _f64p, _f64p]),
+            "orc_pair_path_grad": (None, [_f32p, _f32p, _i64, _int, _int, _int, _int, _u32p, _u32p,
+                                          _f32p, _f64p, _f64p, _f64p, _i32p]),
             "orc_max_threads": (_int, []),
         }
         for name, (res, args) in sigs.items():
@@ -226,3 +234,56 @@ def ucr_ed(x: np.ndarray, q: np.ndarray):
         x.astype(np.float64).tofile(xp)
         q.astype(np.float64).tofile(qp)
         return _run_ucr("UCR_ED_BIN", [xp, qp, str(q.size), str(x.size)])
+
+
+def pair_fwdbwd(q, s, W: int, euclid: bool = True, znorm: bool = True, f32: bool = False,
+                dD=None):
+    """Pairwise cDTW forward/backward (orc_pair_fwdbwd).  q, s: (n, L) float32.
+    Returns D (n,), dq (n, L), ds (n, L), margin (n,)."""
+    q = np.ascontiguousarray(q, dtype=np.float32)
+    s = np.ascontiguousarray(s, dtype=np.float32)
+    n, L = q.shape
+    D = np.empty(n)
+    dq = np.empty((n, L))
+    ds = np.empty((n, L))
+    mg = np.empty(n)
+    up = None if dD is None else np.ascontiguousarray(dD, dtype=np.float32)
+    lib().orc_pair_fwdbwd(_p(q, _f32p), _p(s, _f32p), n, L, W, int(euclid), int(znorm), int(f32),
+                          None if up is None else _p(up, _f32p), _p(D, _f64p), _p(dq, _f64p),
+                          _p(ds, _f64p), _p(mg, _f64p))
+    return D, dq, ds, mg
+
+
+def pair_fwdbwd64(q, s, W: int, euclid: bool = True, znorm: bool = True):
+    """FP64 forward/backward on float64 inputs (orc_pair_fwdbwd64), for
+    finite-difference checks.  Returns D, dq, ds, margin."""
+    q = np.ascontiguousarray(q, dtype=np.float64)
+    s = np.ascontiguousarray(s, dtype=np.float64)
+    n, L = q.shape
+    D = np.empty(n)
+    dq = np.empty((n, L))
+    ds = np.empty((n, L))
+    mg = np.empty(n)
+    lib().orc_pair_fwdbwd64(_p(q, _f64p), _p(s, _f64p), n, L, W, int(euclid), int(znorm),
+                            _p(D, _f64p), _p(dq, _f64p), _p(ds, _f64p), _p(mg, _f64p))
+    return D, dq, ds, mg
+
+
+def pair_path_grad(q, s, W: int, rows, cols, euclid: bool = True, znorm: bool = True, dD=None):
+    """FP64 cost and gradient along a given path (device path-record runs).
+    Returns cost (n,), dq, ds (n, L), valid (n,) bool."""
+    q = np.ascontiguousarray(q, dtype=np.float32)
+    s = np.ascontiguousarray(s, dtype=np.float32)
+    rows = np.ascontiguousarray(rows, dtype=np.uint32)
+    cols = np.ascontiguousarray(cols, dtype=np.uint32)
+    n, L = q.shape
+    cost = np.empty(n)
+    dq = np.empty((n, L))
+    ds = np.empty((n, L))
+    ok = np.empty(n, np.int32)
+    up = None if dD is None else np.ascontiguousarray(dD, dtype=np.float32)
+    lib().orc_pair_path_grad(_p(q, _f32p), _p(s, _f32p), n, L, W, int(euclid), int(znorm),
+                             _p(rows, _u32p), _p(cols, _u32p),
+                             None if up is None else _p(up, _f32p), _p(cost, _f64p),
+                             _p(dq, _f64p), _p(ds, _f64p), _p(ok, _i32p))
+    return cost, dq, ds, ok.astype(bool)

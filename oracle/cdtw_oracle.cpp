@@ -374,6 +374,254 @@ void orc_cdtw_ref_f32(const float* zq, int M, const float* x, const float* avg,
     }
 }
 
+// ---- pairwise cDTW forward / backward (no reference counterpart) ----------
+//
+// The banded DP of banded_dtw above on two equal-length series, with the
+// predecessor kept per cell: diagonal if it is the minimum, else (i-1, j) if
+// it is <= (i, j-1), else (i, j-1).  Backtracking from (L-1, L-1) gives the
+// warping path; the (sub)gradient of D = sum over the path of cost(zq_i - zs_j)
+// is the sum of cost'(zq_i - zs_j) over the path cells of row i (query) or
+// column j (subject, negated), then through the z-normalisation
+// z = (x - mu) / sigma: dx = (g - mean(g) - z * mean(g z)) / sigma
+// (sigma = 1 and no z term when the variance is not positive).
+//
+// f32 = 1 replays the device arithmetic: float DP with one fused
+// multiply-add per cell (|d| + m for the absolute cost), float gradient sums
+// in ascending order along each run.  f32 = 0 is FP64 throughout.
+// margin[p] = smallest gap (second-best minus best predecessor, relative to
+// the best) over the path cells: where it is tiny a float DP may pick another
+// path of (almost) equal cost.
+}  // extern "C"
+
+namespace {
+
+template <class T, class X>
+void pair_one(const X* q, const X* s, int L, int W, bool euclid, bool zn, float up_grad,
+              double* Dout, double* dq, double* ds, double* margin) {
+    const T inf = std::numeric_limits<T>::infinity();
+    std::vector<T> a(L), b(L);
+    double muq = 0, sdq = 1, mus = 0, sds = 1;
+    bool degq = false, degs = false;
+    auto norm = [&](const X* x, std::vector<T>& z, double& mu, double& sd, bool& deg) {
+        double s1 = 0.0;
+        for (int t = 0; t < L; ++t) s1 += (double)x[t];
+        mu = s1 / L;
+        double s2 = 0.0;
+        for (int t = 0; t < L; ++t) s2 += sq((double)x[t] - mu);
+        const double var = s2 / L;
+        deg = !(var > 0.0);
+        sd = deg ? 1.0 : std::sqrt(var);
+        const double inv = 1.0 / sd;
+        for (int t = 0; t < L; ++t) z[t] = (T)(((double)x[t] - mu) * inv);
+    };
+    if (zn) {
+        norm(q, a, muq, sdq, degq);
+        norm(s, b, mus, sds, degs);
+    } else {
+        for (int t = 0; t < L; ++t) {
+            a[t] = (T)q[t];
+            b[t] = (T)s[t];
+        }
+    }
+    const int w2 = 2 * W + 1;
+    std::vector<T> Dt((size_t)L * w2, inf);
+    std::vector<unsigned char> dir((size_t)L * w2, 0);
+    auto at = [&](int i, int j) -> T {
+        if (i < 0 || j < 0 || j - i > W || i - j > W) return inf;
+        return Dt[(size_t)i * w2 + (j - i + W)];
+    };
+    for (int i = 0; i < L; ++i) {
+        for (int j = std::max(0, i - W); j <= std::min(L - 1, i + W); ++j) {
+            const T diag = (i == 0 && j == 0) ? (T)0 : at(i - 1, j - 1);
+            const T upv = at(i - 1, j), left = at(i, j - 1);
+            const T m = std::min(diag, std::min(upv, left));
+            T v;
+            if (sizeof(T) == 4) {
+                const float df = (float)a[i] - (float)b[j];
+                v = euclid ? (T)std::fmaf(df, df, (float)m) : (T)(std::fabs(df) + (float)m);
+            } else {
+                const double df = (double)a[i] - (double)b[j];
+                v = euclid ? (T)(df * df + (double)m) : (T)(std::fabs(df) + (double)m);
+            }
+            Dt[(size_t)i * w2 + (j - i + W)] = v;
+            dir[(size_t)i * w2 + (j - i + W)] = diag == m ? 0 : (upv <= left ? 1 : 2);
+        }
+    }
+    *Dout = (double)at(L - 1, L - 1);
+    // backtrack: row runs [ra, rb], column runs [ca, cb]
+    std::vector<int> ra(L), rb(L), ca(L), cb(L);
+    int i = L - 1, j = L - 1;
+    rb[i] = j;
+    cb[j] = i;
+    double mg = kInf;
+    while (!(i == 0 && j == 0)) {
+        const T diag = at(i - 1, j - 1), upv = at(i - 1, j), left = at(i, j - 1);
+        T v3[3] = {diag, upv, left};
+        std::sort(v3, v3 + 3);
+        if (v3[1] < inf) mg = std::min(mg, ((double)v3[1] - (double)v3[0]) / std::max((double)v3[0], 1e-300));
+        const int d = dir[(size_t)i * w2 + (j - i + W)];
+        if (d == 0) {
+            ra[i] = j;
+            ca[j] = i;
+            --i;
+            --j;
+            rb[i] = j;
+            cb[j] = i;
+        } else if (d == 1) {
+            ra[i] = j;
+            --i;
+            rb[i] = j;
+        } else {
+            ca[j] = i;
+            --j;
+            cb[j] = i;
+        }
+    }
+    ra[0] = 0;
+    ca[0] = 0;
+    *margin = mg;
+    auto fp = [&](T df) -> T {
+        return euclid ? (T)2 * df : (df > 0 ? (T)1 : (df < 0 ? (T)-1 : (T)0));
+    };
+    for (int side = 0; side < 2; ++side) {
+        double* out = side == 0 ? dq : ds;
+        std::vector<T> g(L);
+        for (int t = 0; t < L; ++t) {
+            T acc = 0;
+            const int lo = side == 0 ? ra[t] : ca[t], hi = side == 0 ? rb[t] : cb[t];
+            for (int u = lo; u <= hi; ++u)
+                acc += side == 0 ? fp(a[t] - b[u]) : -fp(a[u] - b[t]);
+            g[t] = acc;
+        }
+        const std::vector<T>& z = side == 0 ? a : b;
+        if (!zn) {
+            for (int t = 0; t < L; ++t) out[t] = (double)(g[t] * (T)up_grad);
+            continue;
+        }
+        double sg = 0.0, sgz = 0.0;
+        for (int t = 0; t < L; ++t) {
+            sg += (double)g[t];
+            sgz += (double)g[t] * (double)z[t];
+        }
+        const bool deg = side == 0 ? degq : degs;
+        const double sd = side == 0 ? sdq : sds;
+        const double m1 = sg / L, m2 = deg ? 0.0 : sgz / L;
+        for (int t = 0; t < L; ++t)
+            out[t] = (double)up_grad * ((double)g[t] - m1 - (double)z[t] * m2) / sd;
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+void orc_pair_fwdbwd(const float* q, const float* s, int64_t n, int L, int W, int euclid,
+                     int znorm, int f32, const float* dD, double* D, double* dq, double* ds,
+                     double* margin) {
+    W = std::max(0, std::min(W, L - 1));
+#pragma omp parallel for schedule(dynamic, 4)
+    for (int64_t p = 0; p < n; ++p) {
+        const float up = dD ? dD[p] : 1.0f;
+        if (f32)
+            pair_one<float, float>(q + p * L, s + p * L, L, W, euclid != 0, znorm != 0, up, D + p,
+                            dq + p * L, ds + p * L, margin + p);
+        else
+            pair_one<double, float>(q + p * L, s + p * L, L, W, euclid != 0, znorm != 0, up, D + p,
+                             dq + p * L, ds + p * L, margin + p);
+    }
+}
+
+// FP64 cost and gradient along a GIVEN warping path (row runs rows[i] =
+// a_i | b_i << 16, column runs cols[j] = c_j | d_j << 16, the device path
+// record): checks that a device path is optimal and that its gradient is the
+// derivative of the cost along it.  Returns per pair 1 if the runs form a
+// monotone connected path from (0, 0) to (L-1, L-1) inside the band, else 0.
+void orc_pair_path_grad(const float* q, const float* s, int64_t n, int L, int W, int euclid,
+                        int znorm, const uint32_t* rows, const uint32_t* cols, const float* dD,
+                        double* cost, double* dq, double* ds, int* valid) {
+    W = std::max(0, std::min(W, L - 1));
+#pragma omp parallel for schedule(dynamic, 4)
+    for (int64_t p = 0; p < n; ++p) {
+        const float* x = q + p * L;
+        const float* y = s + p * L;
+        const uint32_t* R = rows + p * L;
+        const uint32_t* Cc = cols + p * L;
+        std::vector<double> a(L), b(L);
+        double sd[2] = {1, 1};
+        bool deg[2] = {false, false};
+        for (int side = 0; side < 2; ++side) {
+            const float* v = side ? y : x;
+            std::vector<double>& z = side ? b : a;
+            if (!znorm) {
+                for (int t = 0; t < L; ++t) z[t] = v[t];
+                continue;
+            }
+            double s1 = 0;
+            for (int t = 0; t < L; ++t) s1 += v[t];
+            const double mu = s1 / L;
+            double s2 = 0;
+            for (int t = 0; t < L; ++t) s2 += sq(v[t] - mu);
+            deg[side] = !(s2 / L > 0.0);
+            sd[side] = deg[side] ? 1.0 : std::sqrt(s2 / L);
+            for (int t = 0; t < L; ++t) z[t] = (v[t] - mu) / sd[side];
+        }
+        bool ok = true;
+        double c = 0;
+        for (int i = 0; i < L && ok; ++i) {
+            const int lo = (int)(R[i] & 0xffff), hi = (int)(R[i] >> 16);
+            ok = lo <= hi && hi < L && std::abs(i - lo) <= W && std::abs(i - hi) <= W;
+            if (i == 0) ok = ok && lo == 0;
+            if (i == L - 1) ok = ok && hi == L - 1;
+            if (i > 0) {
+                const int phi = (int)(R[i - 1] >> 16);
+                ok = ok && (lo == phi || lo == phi + 1);
+            }
+            for (int j = lo; ok && j <= hi; ++j) {
+                const double d = a[i] - b[j];
+                c += euclid ? d * d : std::fabs(d);
+                // the column runs must describe the same cells
+                const int clo = (int)(Cc[j] & 0xffff), chi = (int)(Cc[j] >> 16);
+                ok = clo <= i && i <= chi;
+            }
+        }
+        valid[p] = ok ? 1 : 0;
+        cost[p] = c;
+        const double up = dD ? dD[p] : 1.0;
+        auto fp = [&](double d) { return euclid ? 2 * d : (d > 0 ? 1.0 : (d < 0 ? -1.0 : 0.0)); };
+        for (int side = 0; side < 2; ++side) {
+            double* out = (side ? ds : dq) + p * L;
+            const uint32_t* run = side ? Cc : R;
+            const std::vector<double>& z = side ? b : a;
+            std::vector<double> g(L, 0.0);
+            for (int t = 0; t < L && ok; ++t) {
+                const int lo = (int)(run[t] & 0xffff), hi = (int)(run[t] >> 16);
+                for (int u = lo; u <= std::min(hi, L - 1); ++u)
+                    g[t] += side ? -fp(a[u] - b[t]) : fp(a[t] - b[u]);
+            }
+            double sg = 0, sgz = 0;
+            for (int t = 0; t < L; ++t) {
+                sg += g[t];
+                sgz += g[t] * z[t];
+            }
+            const double m1 = znorm ? sg / L : 0.0;
+            const double m2 = (znorm && !deg[side]) ? sgz / L : 0.0;
+            for (int t = 0; t < L; ++t) out[t] = up * (g[t] - m1 - z[t] * m2) / sd[side];
+        }
+    }
+}
+
+// FP64 forward/backward on double inputs: the finite-difference pin of the
+// backtracking gradient (central differences need steps far below float
+// resolution).
+void orc_pair_fwdbwd64(const double* q, const double* s, int64_t n, int L, int W, int euclid,
+                       int znorm, double* D, double* dq, double* ds, double* margin) {
+    W = std::max(0, std::min(W, L - 1));
+#pragma omp parallel for schedule(dynamic, 4)
+    for (int64_t p = 0; p < n; ++p)
+        pair_one<double, double>(q + p * L, s + p * L, L, W, euclid != 0, znorm != 0, 1.0f, D + p,
+                                 dq + p * L, ds + p * L, margin + p);
+}
+
 int orc_max_threads(void) { return omp_get_max_threads(); }
 
 }  // extern "C"

@@ -102,3 +102,55 @@ def test_synthetic_generators_deterministic():
     assert a.dtype == np.float32 and np.array_equal(a, b)
     m = synth.metal_like(300000, seed=1)
     assert np.abs(m).max() > 100  # level-shifted regime
+
+
+def _walks(rng, n, L):
+    return np.cumsum(rng.standard_normal((n, L)), axis=1)
+
+
+@pytest.mark.parametrize("euclid", [True, False])
+def test_pair_gradient_oracle_matches_central_differences(euclid):
+    """The backtracking (sub)gradient of the pairwise cDTW through the
+    z-normalisation equals central differences (h = 1e-6, FP64 inputs) at
+    points whose optimal path is stable (path margin well above h)."""
+    rng = np.random.default_rng(11)
+    n, L, W = 6, 40, 5
+    q, s = _walks(rng, n, L), _walks(rng, n, L)
+    D, dq, ds, mg = oracle.pair_fwdbwd64(q, s, W, euclid=euclid)
+    h = 1e-6
+    checked = 0
+    for p in range(n):
+        if mg[p] < 1e-5:
+            continue
+        for t in range(0, L, 5):
+            for side, g in ((0, dq), (1, ds)):
+                a, b = q[p:p + 1].copy(), s[p:p + 1].copy()
+                x = a if side == 0 else b
+                x[0, t] += h
+                dp = oracle.pair_fwdbwd64(a, b, W, euclid=euclid)[0][0]
+                x[0, t] -= 2 * h
+                dm = oracle.pair_fwdbwd64(a, b, W, euclid=euclid)[0][0]
+                fd = (dp - dm) / (2 * h)
+                assert abs(fd - g[p, t]) <= 1e-5 * (1 + abs(g[p, t])), (p, t, side, fd, g[p, t])
+                checked += 1
+    assert checked >= 64
+
+
+def test_pair_oracle_properties():
+    """D equals the banded DTW of the z-normalised pair; the z-normalised
+    gradient is orthogonal to the constant vector and to z (shift and scale
+    invariance); without z-normalisation the squared-cost gradient satisfies
+    Euler's relation <z, g> = 2 D (degree-2 homogeneity)."""
+    rng = np.random.default_rng(12)
+    n, L, W = 4, 64, 9
+    q, s = _walks(rng, n, L).astype(np.float32), _walks(rng, n, L).astype(np.float32)
+    D, dq, ds, _ = oracle.pair_fwdbwd(q, s, W)
+    for p in range(n):
+        a, b = oracle.znorm(q[p].astype(np.float64)), oracle.znorm(s[p].astype(np.float64))
+        assert D[p] == pytest.approx(oracle.cdtw_pair(b, a, W), rel=1e-12)
+        assert abs(dq[p].sum()) < 1e-9 and abs(ds[p].sum()) < 1e-9
+        assert abs(dq[p] @ (q[p] - q[p].mean())) < 1e-6 * np.abs(q[p]).max() * L
+    zq, zs = q / 10, s / 10
+    D, dq, ds, _ = oracle.pair_fwdbwd(zq, zs, W, znorm=False)
+    for p in range(n):
+        assert zq[p] @ dq[p] + zs[p] @ ds[p] == pytest.approx(2 * D[p], rel=1e-9)
