@@ -11,7 +11,7 @@
 // of a lane's cells move by one position every second step and the subject
 // values every other step; the windows are rotated by index (the step loop
 // is unrolled 2C times) and refilled by a shuffle from the neighbouring lane,
-// the edge lanes reading the pair's z-normalised series from shared memory.
+// the edge lanes reading the pair's series from global memory (L2-resident).
 //
 // With a path record the forward also stores 2 bits per band cell (diagonal
 // predecessor is the minimum; up <= left) in device scratch and, once the
@@ -20,6 +20,8 @@
 // sums the cost derivatives over those runs and applies the z-normalisation
 // Jacobian (I - 11'/L - zz'/L) / sigma.
 #include "common.cuh"
+
+#include <utility>
 
 namespace cdtw {
 
@@ -47,6 +49,40 @@ __device__ __forceinline__ float pair_z(float x, double mu, double inv) {
     return (float)(((double)x - mu) * inv);
 }
 
+// Direction bits of one cell, as predicated ORs of immediates: bit SH when
+// the diagonal is the minimum, bit SH+1 when up <= left.
+template <int SH>
+__device__ __forceinline__ void dir_bits(uint32_t& w, float diag, float m, float up, float left) {
+    asm("{\n\t.reg .pred p;\n\tsetp.eq.f32 p, %1, %2;\n\t@p or.b32 %0, %0, %3;\n\t}"
+        : "+r"(w) : "f"(diag), "f"(m), "n"(1u << SH));
+    asm("{\n\t.reg .pred p;\n\tsetp.le.f32 p, %1, %2;\n\t@p or.b32 %0, %0, %3;\n\t}"
+        : "+r"(w) : "f"(up), "f"(left), "n"(2u << SH));
+}
+
+// One cell (compile-time slot c) of an anti-diagonal of parity E.
+template <int C, bool EU, bool DIRS, int E, int RQ, int RS, int c>
+__device__ __forceinline__ void dp_cell(float (&X)[C], const float (&Y)[C], const float (&Q)[C],
+                                        const float (&Sv)[C], const float (&lim)[C], float nb,
+                                        uint32_t& nbits) {
+    const float up = (E == 0) ? Y[c] : (c == C - 1 ? nb : Y[c + 1 < C ? c + 1 : c]);
+    const float left = (E == 0) ? (c == 0 ? nb : Y[c > 0 ? c - 1 : 0]) : Y[c];
+    const float diag = X[c];
+    const float m = min3f(diag, up, left);
+    const float df = __fsub_rn(Q[(c - RQ % C + C) % C], Sv[(c + RS) % C]);
+    float v = EU ? __fmaf_rn(df, df, m) : __fadd_rn(fabsf(df), m);
+    if (E == 1) v = fmaxf(v, lim[c]);  // d = W + 1 lies outside the band
+    X[c] = v;
+    if constexpr (DIRS) dir_bits<2 * c>(nbits, diag, m, up, left);
+}
+
+template <int C, bool EU, bool DIRS, int E, int RQ, int RS, int... Cs>
+__device__ __forceinline__ void dp_cells_seq(float (&X)[C], const float (&Y)[C],
+                                             const float (&Q)[C], const float (&Sv)[C],
+                                             const float (&lim)[C], float nb, uint32_t& nbits,
+                                             std::integer_sequence<int, Cs...>) {
+    (dp_cell<C, EU, DIRS, E, RQ, RS, Cs>(X, Y, Q, Sv, lim, nb, nbits), ...);
+}
+
 // One anti-diagonal of parity E: X (slots of k-2) becomes k from Y (k-1).
 // Logical query value of slot c is Q[(c - RQ) mod C], subject value
 // Sv[(c + RS) mod C].
@@ -55,21 +91,8 @@ __device__ __forceinline__ void dp_cells(float (&X)[C], const float (&Y)[C], con
                                          const float (&Sv)[C], const float (&lim)[C], float nb,
                                          uint32_t& bits) {
     uint32_t nbits = 0;
-#pragma unroll
-    for (int c = 0; c < C; ++c) {
-        const float up = (E == 0) ? Y[c] : (c == C - 1 ? nb : Y[c + 1 < C ? c + 1 : c]);
-        const float left = (E == 0) ? (c == 0 ? nb : Y[c > 0 ? c - 1 : 0]) : Y[c];
-        const float diag = X[c];
-        const float m = min3f(diag, up, left);
-        const float df = __fsub_rn(Q[(c - RQ % C + C) % C], Sv[(c + RS) % C]);
-        float v = EU ? __fmaf_rn(df, df, m) : __fadd_rn(fabsf(df), m);
-        if (E == 1) v = fmaxf(v, lim[c]);  // d = W + 1 lies outside the band
-        X[c] = v;
-        if (DIRS) {
-            nbits |= (diag == m ? 1u : 0u) << (2 * c);
-            nbits |= (up <= left ? 2u : 0u) << (2 * c);
-        }
-    }
+    dp_cells_seq<C, EU, DIRS, E, RQ, RS>(X, Y, Q, Sv, lim, nb, nbits,
+                                         std::make_integer_sequence<int, C>{});
     if (DIRS) bits = (2 * C >= 32) ? nbits : ((bits << (2 * C)) | nbits);
 }
 
@@ -111,7 +134,7 @@ __device__ __forceinline__ void step_odd(PairLane<C>& st, const float* ss, int L
         st.Sv[slot] = (l == G - 1) ? st.ps : v;
         if (l == G - 1) {
             ++st.js;
-            st.ps = st.js + 1 < L ? ss[st.js + 1] : 0.f;
+            st.ps = st.js + 1 < L ? __ldg(ss + st.js + 1) : 0.f;
         }
     }
     float nb = __shfl_down_sync(kFull, st.A[0], 1, G);
@@ -128,7 +151,7 @@ __device__ __forceinline__ void step_even(PairLane<C>& st, const float* sq, int 
         st.Q[slot] = (l == 0) ? st.pq : v;
         if (l == 0) {
             ++st.iq;
-            st.pq = st.iq + 1 < L ? sq[st.iq + 1] : 0.f;
+            st.pq = st.iq + 1 < L ? __ldg(sq + st.iq + 1) : 0.f;
         }
     }
     float nb = __shfl_up_sync(kFull, st.B[C - 1], 1, G);
@@ -154,8 +177,23 @@ __device__ __forceinline__ void body(PairLane<C>& st, const float* sq, const flo
     }
 }
 
+__device__ __forceinline__ void cp_async4(void* dst, const void* src) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+    asm volatile("cp.async.commit_group;" ::: "memory");
+}
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+constexpr int kWalkStages = 4;            // direction chunks in flight during backtracking
+constexpr int kMoveLog = kWalkRows * 16;  // bytes: the moves of one chunk (<= kWalkRows * S)
+
 template <int C, bool EU, bool DIRS>
-__global__ void __launch_bounds__(kPairThreads) pair_fwd_kernel(const PairArgs a) {
+__global__ void __launch_bounds__(kPairThreads, DIRS ? 2 : 4) pair_fwd_kernel(const PairArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
     const int G = a.G, L = a.L, W = a.W;
     const int tid = threadIdx.x;
@@ -164,15 +202,8 @@ __global__ void __launch_bounds__(kPairThreads) pair_fwd_kernel(const PairArgs a
     const int64_t grp = (int64_t)blockIdx.x * (blockDim.x >> a.lgG) + gib;
     const bool live = grp < a.n;
     const int64_t pr = live ? grp : a.n - 1;
-    const size_t gbytes = (size_t)round_up(8 * (int64_t)L + 64 * G, 16);
-    float* sq = (float*)(smem + gib * gbytes);
-    float* ss = sq + L;
-    uint32_t* wbuf = (uint32_t*)(ss + L);  // kWalkRows x G words
-    for (int t = l; t < L; t += G) {
-        sq[t] = __ldg(a.zq + pr * L + t);
-        ss[t] = __ldg(a.zs + pr * L + t);
-    }
-    __syncwarp();
+    const float* sq = a.zq + pr * L;  // the pair's series (L2-resident; edge lanes read them)
+    const float* ss = a.zs + pr * L;
 
     const int K = 2 * L - 1;
     const int e0 = W & 1;
@@ -188,16 +219,16 @@ __global__ void __launch_bounds__(kPairThreads) pair_fwd_kernel(const PairArgs a
         st.B[c] = e0 == 0 ? CDTW_INF : org;
         const int d = -W + 2 * p + e0;
         const int i = -d / 2, j = d / 2;  // k = 0
-        st.Q[c] = (i >= 0 && i < L) ? sq[i] : 0.f;
-        st.Sv[c] = (j >= 0 && j < L) ? ss[j] : 0.f;
+        st.Q[c] = (i >= 0 && i < L) ? __ldg(sq + i) : 0.f;
+        st.Sv[c] = (j >= 0 && j < L) ? __ldg(ss + j) : 0.f;
     }
     st.bits = 0;
     st.u = 0;
     st.kb = 0;
     st.iq = (W - e0) / 2;                      // lane 0's slot-0 query index at k = 0
     st.js = (-W + 2 * (G * C - 1) + e0) / 2;  // lane G-1's last-slot subject index
-    st.pq = (st.iq + 1 < L) ? sq[st.iq + 1] : 0.f;
-    st.ps = (st.js + 1 < L) ? ss[st.js + 1] : 0.f;
+    st.pq = (st.iq + 1 < L) ? __ldg(sq + st.iq + 1) : 0.f;
+    st.ps = (st.js + 1 < L) ? __ldg(ss + st.js + 1) : 0.f;
     uint32_t* drow = DIRS ? a.dirs + (size_t)pr * a.nkb * G : nullptr;
 
     int k = 0;
@@ -217,7 +248,7 @@ __global__ void __launch_bounds__(kPairThreads) pair_fwd_kernel(const PairArgs a
             st.Q[0] = (l == 0) ? st.pq : v;
             if (l == 0) {
                 ++st.iq;
-                st.pq = st.iq + 1 < L ? sq[st.iq + 1] : 0.f;
+                st.pq = st.iq + 1 < L ? __ldg(sq + st.iq + 1) : 0.f;
             }
             step_even<C, EU, DIRS, 0, 0>(st, sq, L, G, l, false);
             flush_bits<C, DIRS>(st, drow, G, l, k, K, live);
@@ -234,73 +265,111 @@ __global__ void __launch_bounds__(kPairThreads) pair_fwd_kernel(const PairArgs a
     if (live && p0 <= porg && porg < p0 + C) a.D[pr] = dval;
     if (!DIRS) return;
 
-    // Backtracking: direction rows staged kWalkRows at a time; lane 0 walks.
-    __syncwarp();
+    // Backtracking: chunks of kWalkRows direction rows stream into a
+    // kWalkStages-deep shared-memory ring (cp.async).  Lane 0 of the group
+    // decodes the moves of a chunk into a byte log (2-bit codes: 1 or 3
+    // diagonal, 2 up (i-1, j), 0 left (i, j-1)); the group then turns the log
+    // into row runs (a_i, b_i) and column runs (c_j, d_j) with a scan.  Cell
+    // (0, 0) always records a diagonal move (its diagonal is the origin, the
+    // other predecessors are +inf): it writes the last runs and ends the walk.
     constexpr int S = 16 / C;
-    uint16_t* prow = (uint16_t*)sq;  // path runs, staged (the series are no longer needed)
-    uint16_t* pcol = prow + 2 * L;
-    int wi = L - 1, wj = L - 1, wk = K - 1;
-    bool done = false;
-    if (l == 0) {
-        prow[2 * wi + 1] = (uint16_t)wj;
-        pcol[2 * wj + 1] = (uint16_t)wi;
-    }
-    for (int rhi = a.nkb - 1; rhi >= 0; rhi -= kWalkRows) {
-        __syncwarp();
+    uint32_t* ring = (uint32_t*)smem + (size_t)gib * kWalkStages * kWalkRows * G;
+    uint8_t* mlog = smem + (size_t)blockDim.x * kWalkStages * kWalkRows * 4 + gib * kMoveLog;
+    const int nch = (a.nkb + kWalkRows - 1) / kWalkRows;
+    auto issue = [&](int ch) {
+        if (ch < nch) {
+            uint32_t* dst = ring + (ch % kWalkStages) * kWalkRows * G;
+            const int rhi = a.nkb - 1 - ch * kWalkRows;
 #pragma unroll 4
-        for (int t = 0; t < kWalkRows; ++t) {
-            const int r = rhi - t;
-            if (r >= 0) wbuf[t * G + l] = drow[(size_t)r * G + l];
+            for (int t = 0; t < kWalkRows; ++t) {
+                const int r = rhi - t;
+                if (r >= 0) cp_async4(dst + t * G + l, drow + (size_t)r * G + l);
+            }
         }
+        cp_async_commit();
+    };
+    __syncwarp();  // the group's direction words are visible to all its lanes
+#pragma unroll
+    for (int ch = 0; ch < kWalkStages - 1; ++ch) issue(ch);
+    uint16_t* r16 = (uint16_t*)(a.rows + pr * L);  // [2i] = a_i, [2i+1] = b_i
+    uint16_t* c16 = (uint16_t*)(a.cols + pr * L);  // [2j] = c_j, [2j+1] = d_j
+    if (l == 0 && live) {
+        r16[2 * (L - 1) + 1] = (uint16_t)(L - 1);
+        c16[2 * (L - 1) + 1] = (uint16_t)(L - 1);
+    }
+    int kb = (K - 1) / S, uu = (K - 1) - kb * S, e = e0;  // walker: anti-diagonal kb*S+uu
+    int lw = porg / C, c = porg - lw * C;                  // slot c of lane lw, parity e
+    int gi = L - 1, gj = L - 1;  // (group-uniform) cell before the chunk's first move
+    for (int ch = 0; ch < nch; ++ch) {  // same trip count in every group of the warp
+        issue(ch + kWalkStages - 1);
+        cp_async_wait<kWalkStages - 1>();
         __syncwarp();
-        if (l == 0) {
-            const int rlo = rhi - kWalkRows + 1;
-            while (!done) {
-                const int kb = wk / S;
-                if (kb < rlo) break;
-                if (wi == 0 && wj == 0) {
-                    prow[0] = 0;
-                    pcol[0] = 0;
-                    done = true;
-                    break;
-                }
-                const int e = (wk + W) & 1;
-                const int p = (wj - wi + W - e) >> 1;
-                const int lw = p / C, c = p - lw * C;
-                const int uu = wk - kb * S;
-                const uint32_t wd = wbuf[(rhi - kb) * G + lw];
+        int nm = 0;
+        if (l == 0 && live) {  // groups past the last pair do not walk
+            const uint32_t* buf = ring + (ch % kWalkStages) * kWalkRows * G;
+            const int rhi = a.nkb - 1 - ch * kWalkRows;
+            const int rlo = max(rhi - kWalkRows + 1, 0);
+            while (kb >= rlo && (unsigned)lw < (unsigned)G && nm < kMoveLog) {
+                const uint32_t wd = buf[(rhi - kb) * G + lw];
                 const uint32_t b = (wd >> (2 * C * (S - 1 - uu) + 2 * c)) & 3u;
-                if (b & 1u) {  // diagonal
-                    prow[2 * wi] = (uint16_t)wj;
-                    pcol[2 * wj] = (uint16_t)wi;
-                    --wi;
-                    --wj;
-                    wk -= 2;
-                    prow[2 * wi + 1] = (uint16_t)wj;
-                    pcol[2 * wj + 1] = (uint16_t)wi;
-                } else if (b & 2u) {  // up: (i-1, j)
-                    prow[2 * wi] = (uint16_t)wj;
-                    --wi;
-                    wk -= 1;
-                    prow[2 * wi + 1] = (uint16_t)wj;
-                } else {  // left: (i, j-1)
-                    pcol[2 * wj] = (uint16_t)wi;
-                    --wj;
-                    wk -= 1;
-                    pcol[2 * wj + 1] = (uint16_t)wi;
+                mlog[nm++] = (uint8_t)b;
+                const bool dg = b & 1u;
+                const int dp = dg ? 0 : (b ? e : e - 1);  // up: d + 1, left: d - 1
+                e ^= dg ? 0 : 1;
+                if (S == 1) {
+                    kb -= 1 + dg;
+                } else {
+                    uu -= 1 + dg;
+                    if (uu < 0) {
+                        uu += S;
+                        --kb;
+                    }
+                }
+                c += dp;
+                if (c >= C) {
+                    c -= C;
+                    ++lw;
+                } else if (c < 0) {
+                    c += C;
+                    --lw;
                 }
             }
         }
-    }
-    __syncwarp();
-    if (live) {
-        const uint32_t* r32 = (const uint32_t*)prow;
-        const uint32_t* c32 = (const uint32_t*)pcol;
-        for (int t = l; t < L; t += G) {
-            a.rows[pr * L + t] = r32[t];
-            a.cols[pr * L + t] = c32[t];
+        nm = __shfl_sync(kFull, nm, 0, G);
+        // every lane of the warp runs the same number of scan rounds (the
+        // groups' move counts differ): the full-mask shuffles below need it
+        const int nmax = __reduce_max_sync(kFull, (unsigned)nm);
+        __syncwarp();
+        for (int m0 = 0; m0 < nmax; m0 += G) {
+            const int m = m0 + l;
+            const uint32_t b = m < nm ? mlog[m] : 2u;
+            const int lr = (m < nm && b != 0u) ? 1 : 0;  // leaves its row
+            const int lc = (m < nm && b != 2u) ? 1 : 0;  // leaves its column
+            int sr = lr, sc = lc;                        // inclusive scans over the group
+            for (int o = 1; o < G; o <<= 1) {
+                const int tr = __shfl_up_sync(kFull, sr, o, G);
+                const int tc = __shfl_up_sync(kFull, sc, o, G);
+                if (l >= o) {
+                    sr += tr;
+                    sc += tc;
+                }
+            }
+            const int ib = gi - (sr - lr), jb = gj - (sc - lc);  // cell before move m
+            const bool inside = live && (unsigned)ib < (unsigned)L && (unsigned)jb < (unsigned)L;
+            if (inside && lr) {
+                r16[2 * ib] = (uint16_t)jb;                               // a_i
+                if (ib > 0) r16[2 * (ib - 1) + 1] = (uint16_t)(jb - lc);  // b_(i-1)
+            }
+            if (inside && lc) {
+                c16[2 * jb] = (uint16_t)ib;                               // c_j
+                if (jb > 0) c16[2 * (jb - 1) + 1] = (uint16_t)(ib - lr);  // d_(j-1)
+            }
+            gi -= __shfl_sync(kFull, sr, G - 1, G);
+            gj -= __shfl_sync(kFull, sc, G - 1, G);
         }
+        __syncwarp();
     }
+    cp_async_wait<0>();
 }
 
 // z-normalisation of every series of the pairs: one warp per series, FP64
@@ -336,61 +405,113 @@ __global__ void pair_znorm_kernel(const float* __restrict__ q, const float* __re
     }
 }
 
-// Backward: one warp per pair.  g_q[i] = sum over the row run of f'(zq_i -
-// zs_j), g_s[j] = -sum over the column run; then through the z-normalisation
-// and scaled by dD.
+// Exclusive FP64 prefix sums P[0..L] of the L floats in x, by one warp
+// (each lane a contiguous slice, then a scan of the slice totals).
+__device__ void warp_prefix(const float* x, double* P, int L, int lane) {
+    const int per = (L + 31) / 32;
+    const int lo = min(lane * per, L), hi = min(lo + per, L);
+    double tot = 0.0;
+    for (int t = lo; t < hi; ++t) tot += (double)x[t];
+    double inc = tot;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const double v = __shfl_up_sync(kFull, inc, o);
+        if (lane >= o) inc += v;
+    }
+    double run = inc - tot;
+    for (int t = lo; t < hi; ++t) {
+        P[t] = run;
+        run += (double)x[t];
+    }
+    if (lane == 31) P[L] = inc;
+    __syncwarp();
+}
+
+// Backward: one warp per pair, the pair's z values staged in shared memory.
+// g_q[i] = sum over the row run [a_i, b_i] of f'(zq_i - zs_j), g_s[j] = -sum
+// over the column run; then through the z-normalisation and scaled by dD.
+// For the squared cost f'(d) = 2d and a run sum is 2 (len zq_i - (P[b+1] -
+// P[a])) with FP64 prefix sums P of the other series: no per-run loop, so
+// lanes with long runs do not hold up the warp.  Runs are clamped to
+// [0, L-1], so a damaged path record cannot index outside the staged series.
 template <bool EU>
-__global__ void pair_bwd_kernel(const float* __restrict__ q, const float* __restrict__ s,
-                                int64_t n, int L, const double* __restrict__ hdr,
-                                const uint32_t* __restrict__ rows,
-                                const uint32_t* __restrict__ cols, const float* __restrict__ dD,
-                                float* __restrict__ dq, float* __restrict__ ds) {
-    const int lane = threadIdx.x & 31;
-    const int64_t pr = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+__global__ void __launch_bounds__(128)
+pair_bwd_kernel(const float* __restrict__ q, const float* __restrict__ s, int64_t n, int L,
+                const double* __restrict__ hdr, const uint32_t* __restrict__ rows,
+                const uint32_t* __restrict__ cols, const float* __restrict__ dD,
+                float* __restrict__ dq, float* __restrict__ ds) {
+    extern __shared__ __align__(16) unsigned char bsm[];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const int64_t pr = (int64_t)blockIdx.x * (blockDim.x >> 5) + wib;
     if (pr >= n) return;
+    // per warp: prefix sums (L+1 doubles, squared cost only), zq, zs (L floats each)
+    const size_t wbytes = (EU ? 8 * (size_t)(L + 1) : 0) + 8 * (size_t)L;
+    double* P = (double*)(bsm + (size_t)wib * round_up((int64_t)wbytes, 16));
+    float* zqs = (float*)(P + (EU ? L + 1 : 0));
+    float* zss = zqs + L;
     const bool zn = hdr != nullptr;
     double muq = 0.0, invq = 1.0, mus = 0.0, invs = 1.0;
     bool degq = false, degs = false;
     if (zn) {
         muq = hdr[pr * 4 + 0];
-        const double sq = hdr[pr * 4 + 1];
+        const double sdq = hdr[pr * 4 + 1];
         mus = hdr[pr * 4 + 2];
-        const double ssd = hdr[pr * 4 + 3];
-        degq = sq < 0.0;
-        degs = ssd < 0.0;
-        invq = 1.0 / (degq ? 1.0 : sq);
-        invs = 1.0 / (degs ? 1.0 : ssd);
+        const double sds = hdr[pr * 4 + 3];
+        degq = sdq < 0.0;
+        degs = sds < 0.0;
+        invq = 1.0 / (degq ? 1.0 : sdq);
+        invs = 1.0 / (degs ? 1.0 : sds);
     }
     const float* xq = q + pr * L;
     const float* xs = s + pr * L;
-    auto zqv = [&](int t) { return zn ? pair_z(__ldg(xq + t), muq, invq) : __ldg(xq + t); };
-    auto zsv = [&](int t) { return zn ? pair_z(__ldg(xs + t), mus, invs) : __ldg(xs + t); };
-    auto fp = [](float df) {
-        return EU ? 2.0f * df : (df > 0.f ? 1.0f : (df < 0.f ? -1.0f : 0.0f));
-    };
+    for (int t = lane; t < L; t += 32) {
+        const float a = __ldg(xq + t), b = __ldg(xs + t);
+        zqs[t] = zn ? pair_z(a, muq, invq) : a;
+        zss[t] = zn ? pair_z(b, mus, invs) : b;
+    }
+    __syncwarp();
+    auto fp = [](float df) { return df > 0.f ? 1.0f : (df < 0.f ? -1.0f : 0.0f); };
     const float up = dD ? __ldg(dD + pr) : 1.0f;
     for (int side = 0; side < 2; ++side) {
         float* out = side == 0 ? dq : ds;
         if (!out) continue;
+        out += pr * L;
         const uint32_t* run = (side == 0 ? rows : cols) + pr * L;
+        const float* zt_s = side == 0 ? zqs : zss;
+        const float* zo_s = side == 0 ? zss : zqs;
+        if (EU) warp_prefix(zo_s, P, L, lane);
         double sg = 0.0, sgz = 0.0;
-        for (int t = lane; t < L; t += 32) {
-            const uint32_t r = __ldg(run + t);
-            const int lo = (int)(r & 0xffffu), hi = (int)(r >> 16);
-            const float zt = side == 0 ? zqv(t) : zsv(t);
-            float g = 0.f;
-            for (int u = lo; u <= hi; ++u) {
-                const float other = side == 0 ? zsv(u) : zqv(u);
-                g += side == 0 ? fp(__fsub_rn(zt, other)) : -fp(__fsub_rn(other, zt));
+        for (int t0 = lane; t0 < L; t0 += 4 * 32) {
+            uint32_t r[4];  // four runs in flight per lane
+#pragma unroll
+            for (int v = 0; v < 4; ++v) r[v] = t0 + 32 * v < L ? __ldg(run + t0 + 32 * v) : 0u;
+#pragma unroll
+            for (int v = 0; v < 4; ++v) {
+                const int t = t0 + 32 * v;
+                if (t >= L) break;
+                const int hi = min((int)(r[v] >> 16), L - 1);
+                const int lo = min((int)(r[v] & 0xffffu), hi);
+                const float zt = zt_s[t];
+                float g;
+                if (EU) {
+                    // q side: sum_j 2 (zq_t - zs_j); s side: -sum_i 2 (zq_i - zs_t)
+                    // = sum_i 2 (zs_t - zq_i): both 2 (len z_t - sum of the other)
+                    const double sum = (double)(hi - lo + 1) * (double)zt - (P[hi + 1] - P[lo]);
+                    g = (float)(2.0 * sum);
+                } else {
+                    g = 0.f;
+                    for (int u = lo; u <= hi; ++u) {
+                        const float o = zo_s[u];
+                        g += side == 0 ? fp(__fsub_rn(zt, o)) : -fp(__fsub_rn(o, zt));
+                    }
+                }
+                out[t] = zn ? g : g * up;
+                sg += (double)g;
+                sgz += (double)g * (double)zt;
             }
-            out[pr * L + t] = g;
-            sg += (double)g;
-            sgz += (double)g * (double)zt;
         }
-        if (!zn) {
-            for (int t = lane; t < L; t += 32) out[pr * L + t] *= up;
-            continue;
-        }
+        __syncwarp();  // P is rebuilt for the other side
+        if (!zn) continue;
         for (int o = 16; o > 0; o >>= 1) {
             sg += __shfl_xor_sync(kFull, sg, o);
             sgz += __shfl_xor_sync(kFull, sgz, o);
@@ -398,12 +519,8 @@ __global__ void pair_bwd_kernel(const float* __restrict__ q, const float* __rest
         const bool deg = side == 0 ? degq : degs;
         const double inv = side == 0 ? invq : invs;
         const double mg = sg / (double)L, mgz = deg ? 0.0 : sgz / (double)L;
-        __syncwarp();
-        for (int t = lane; t < L; t += 32) {
-            const double g = (double)out[pr * L + t];
-            const double zt = (double)(side == 0 ? zqv(t) : zsv(t));
-            out[pr * L + t] = (float)((double)up * (g - mg - zt * mgz) * inv);
-        }
+        for (int t = lane; t < L; t += 32)  // each lane re-reads its own values
+            out[t] = (float)((double)up * ((double)out[t] - mg - (double)zt_s[t] * mgz) * inv);
     }
 }
 
@@ -439,13 +556,12 @@ PairFwdK fwd_kernel(int C, bool eu, bool dirs) {
 }  // namespace
 
 // Lanes per pair (G, a power of two) and band slots per lane (C): about four
-// cells per lane for short bands, 32 lanes for long ones, and G large enough
-// that a warp's staged series fit in 48 KB of shared memory.
+// cells per lane for short bands, 32 lanes for long ones.
 void pair_shape(int L, int W, int* G, int* C) {
+    (void)L;
     const int slots = W + 1;
     int g = 1;
     while (g < 32 && (slots + g - 1) / g > 4) g *= 2;
-    while (g < 32 && (int64_t)(32 / g) * (8 * (int64_t)L + 64 * g) > 49152) g *= 2;
     *G = g;
     *C = (slots + g - 1) / g;
 }
@@ -486,11 +602,10 @@ int launch_pair_fwd(cdtw_handle h, const float* zq, const float* zs, int64_t n, 
     a.nkb = (int)div_up(2 * (int64_t)L - 1, 16 / C);
     a.rows = rows;
     a.cols = cols;
-    const size_t gbytes = (size_t)round_up(8 * (int64_t)L + 64 * G, 16);
-    // threads per block: up to 128, fewer when a long series leaves no room
-    int threads = kPairThreads;
-    while (threads > 32 && (size_t)(threads / G) * gbytes > 160 * 1024) threads /= 2;
-    const size_t smem = (size_t)(threads / G) * gbytes;
+    const int threads = kPairThreads;
+    // backtracking ring (kWalkStages x kWalkRows words per lane) + move log per group
+    const size_t smem =
+        dirs ? (size_t)threads * kWalkStages * kWalkRows * 4 + (size_t)(threads / G) * kMoveLog : 0;
     const int64_t groups_per_block = threads / G;
     const int64_t blocks = div_up(n, groups_per_block);
     if (blocks > INT32_MAX) return set_error(h, CDTW_EINVAL, "too many pairs");
@@ -505,11 +620,17 @@ int launch_pair_fwd(cdtw_handle h, const float* zq, const float* zs, int64_t n, 
 int launch_pair_bwd(cdtw_handle h, const float* q, const float* s, int64_t n, int L,
                     const double* hdr, const uint32_t* rows, const uint32_t* cols,
                     const float* dD, bool euclid, float* dq, float* ds) {
-    const int blocks = (int)div_up(n * 32, 128);
-    if (euclid)
-        pair_bwd_kernel<true><<<blocks, 128, 0, h->stream>>>(q, s, n, L, hdr, rows, cols, dD, dq, ds);
-    else
-        pair_bwd_kernel<false><<<blocks, 128, 0, h->stream>>>(q, s, n, L, hdr, rows, cols, dD, dq, ds);
+    // per warp: z of both series (8L bytes) and, for the squared cost, one
+    // prefix-sum array (8(L+1) bytes); up to 4 warps in 96 KB
+    const size_t wbytes =
+        (size_t)round_up((int64_t)((euclid ? 8 * (size_t)(L + 1) : 0) + 8 * (size_t)L), 16);
+    const int nw = (int)std::max<size_t>(1, std::min<size_t>(4, 96 * 1024 / wbytes));
+    const size_t smem = (size_t)nw * wbytes;
+    const int blocks = (int)div_up(n, nw);
+    auto k = euclid ? pair_bwd_kernel<true> : pair_bwd_kernel<false>;
+    CDTW_CUDA(h, cudaFuncSetAttribute((const void*)k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)smem));
+    k<<<blocks, nw * 32, smem, h->stream>>>(q, s, n, L, hdr, rows, cols, dD, dq, ds);
     CDTW_LAUNCH(h, "pair_bwd_kernel");
     return CDTW_OK;
 }
