@@ -288,6 +288,8 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
                              "peak_source": "measured: cdtw_calibrate_cell_rate (FADD+FMNMX3+FFMA"
                                             " chains) on this GPU in this run"},
                 "argmin": {str(w): b for w, b in zip(bands, best)}, "cut_offset": off}
+        if world == 1 and not args.no_sub:
+            line["subresults"] = subresults(h, dev)
         if world == 1:
             g, thr, n, dt = cpu_port_gcups(x, q, bands, 10.0)
             line["cpu_baseline"] = {
@@ -296,6 +298,130 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
                           f"restatement of openmp_cdtw, {dt:.1f}s"}
         print(json.dumps(line), flush=True)
     h.close()
+
+
+def subresults(h, dev) -> dict:
+    """The other scope rows, measured beside the headline (one GPU, rank 0).
+
+    * pruned_search: config 0 (2^20 ECG-like, M=128, W=12) and config 1
+      (2^25 metal-like, M in {128,256,512,1024} x P in {5,10,20}): device time
+      of one full search (statistics excluded; they are shared per M),
+      effective GCUPS = windows * cells(M,W) / time, stream samples/s.
+    * batched_search: a 128-query sample of config 2 (2^24 ECG-like stream,
+      M ~ U{64..1024}, P in {5,10,20}) as one batched graph call, against the
+      same queries as 128 plain searches on the same GPU.
+    * pair_fwd_bwd: config 3 (4096 pairs, L=256, W=25, z-normalised random
+      walks) and its L=2048/W=409 variant: forward (D only), forward with the
+      path record, backward, and their ratio; CUDA-graph replays, device time.
+    """
+    import torch
+    from cudadtw_b200 import synth
+    out = {}
+    stream = torch.cuda.current_stream(dev)
+
+    def dev_time(fn, reps=1):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(reps):
+            r = fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / 1e3 / reps, r
+
+    # -- pruned search -----------------------------------------------------
+    rows = []
+    cases = [("config0 ecg 2^20", synth.ecg_like(1 << 20, seed=0), [(128, 10)], 0.05)]
+    cases.append(("config1 metal 2^25", synth.metal_like(1 << 25, seed=1),
+                  [(m, p) for m in (128, 256, 512, 1024) for p in (5, 10, 20)], 0.1))
+    for name, x, qs, noise in cases:
+        dx = torch.from_numpy(x).to(dev)
+        for m, pct in qs:
+            q, off = synth.cut_query(x, m, seed=100 + m + pct, noise=noise)
+            w = synth.band_from_percent(m, pct)
+            avg, std = h.avg_std(dx, m)
+            h.set_query(q, w)
+            h.prune_cdtw(dx, avg, std)  # warm
+            t, (loc, dist) = dev_time(lambda: h.prune_cdtw(dx, avg, std))
+            nwin = x.size - m + 1
+            rows.append({"case": name, "M": m, "P": pct, "W": w, "ms": t * 1e3,
+                         "effective_gcups": nwin * cells(m, w) / t / 1e9,
+                         "samples_per_s": nwin / t, "location": int(loc),
+                         "planted": int(off), "counts": list(h.search_counts())})
+        del dx
+    out["pruned_search"] = rows
+
+    # -- batched vs plain ----------------------------------------------------
+    x = synth.ecg_like(1 << 24, seed=0)
+    dx = torch.from_numpy(x).to(dev)
+    batch = synth.batch_queries(x, 512)[::4]  # every 4th of the 512: 128 queries
+    qs = [b[0] for b in batch]
+    ws = [b[1] for b in batch]
+    h.search_batched(dx, qs, ws)  # builds and replays the graph once
+    tb, (bl, bd) = dev_time(lambda: h.search_batched(dx, qs, ws))
+    stats = {}
+    for m in sorted({q.size for q in qs}):
+        stats[m] = h.avg_std(dx, m)
+
+    def plain():
+        res = []
+        for q, w in zip(qs, ws):
+            avg, std = stats[q.size]
+            h.set_query(q, w)
+            res.append(h.prune_cdtw(dx, avg, std))
+        return res
+    tp, pres = dev_time(plain)
+    same = sum(int(a == r[0]) for a, r in zip(bl, pres))
+    out["batched_search"] = {"queries": len(qs), "stream": "ecg 2^24", "batched_s": tb,
+                             "plain_s": tp, "speedup": tp / tb, "same_location": same,
+                             "note": "plain excludes the per-length statistics (shared)"}
+    del dx
+
+    # -- pair forward / backward ------------------------------------------
+    pair = {}
+    for n, L, W in ((4096, 256, 25), (4096, 2048, 409)):
+        rng = np.random.default_rng(3)
+        q = torch.from_numpy(np.cumsum(rng.standard_normal((n, L)), 1).astype(np.float32)).to(dev)
+        s = torch.from_numpy(np.cumsum(rng.standard_normal((n, L)), 1).astype(np.float32)).to(dev)
+        path = torch.empty(h.pair_path_bytes(n, L), dtype=torch.uint8, device=dev)
+        D = torch.empty(n, device=dev)
+        gq, gs = torch.empty_like(q), torch.empty_like(s)
+        fns = {"fwd": lambda: h.pair_fwd(q, s, W, out=D),
+               "fwd_path": lambda: h.pair_fwd(q, s, W, path=path, out=D),
+               "bwd": lambda: h.pair_bwd(q, s, path, dq=gq, ds=gs)}
+        fns["fwd_bwd"] = lambda: (fns["fwd_path"](), fns["bwd"]())
+        r = {}
+        side = torch.cuda.Stream(dev)
+        h.use_torch_stream(side)
+        with torch.cuda.stream(side):
+            for k, f in fns.items():
+                for _ in range(3):
+                    f()
+                torch.cuda.synchronize()
+                g = torch.cuda.CUDAGraph()
+                with torch.cuda.graph(g, stream=side):
+                    for _ in range(10):
+                        f()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                g.replay()
+                torch.cuda.synchronize()
+                e0.record(side)
+                g.replay()
+                e1.record(side)
+                torch.cuda.synchronize()
+                r[k + "_ms"] = e0.elapsed_time(e1) / 10
+                del g
+        h.use_torch_stream(stream)
+        c = cells(L, W)
+        r["fwd_gcups"] = n * c / (r["fwd_ms"] / 1e3) / 1e9
+        r["fwd_bwd_over_fwd"] = r["fwd_bwd_ms"] / r["fwd_ms"]
+        r["bytes_per_pair"] = {"path_record": h.pair_path_bytes(1, L),
+                               "direction_scratch": h.pair_workspace_bytes(1, L, W, False, True),
+                               "full_fp32_band_table": 4 * c}
+        pair[f"{n}x{L}_W{W}"] = r
+        del q, s, path, gq, gs
+    out["pair_fwd_bwd"] = pair
+    return out
 
 
 def ctypes_peak(lib, h) -> float:
@@ -313,6 +439,8 @@ def main() -> None:
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-sub", action="store_true",
+                    help="skip the pruned / batched search and pair fwd/bwd sub-results")
     ap.add_argument("--only-kernels", action="store_true",
                     help="device-timed steps only (no calibration, e2e or CPU baseline): "
                          "the target of ncu captures")

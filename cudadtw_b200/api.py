@@ -281,6 +281,12 @@ class Handle:
         """Bytes of the path record cdtw_pair_fwd writes for n pairs of length L."""
         return int(self._lib.cdtw_pair_path_bytes(n, L))
 
+    def pair_workspace_bytes(self, n: int, L: int, W: int, znorm: bool = True,
+                             with_path: bool = True) -> int:
+        """Device work memory pair_fwd takes from the handle's workspace."""
+        return int(self._lib.cdtw_pair_workspace_bytes(n, L, W, self.PAIR_ZNORM if znorm else 0,
+                                                       int(with_path)))
+
     def pair_fwd(self, q: torch.Tensor, s: torch.Tensor, W: int, metric=EUCLIDEAN,
                  znorm: bool = True, path: torch.Tensor | None = None,
                  out: torch.Tensor | None = None) -> torch.Tensor:

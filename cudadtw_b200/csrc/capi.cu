@@ -492,6 +492,19 @@ size_t cdtw_pair_path_bytes(int64_t n, int L) {
     return (size_t)n * 32 + (size_t)n * L * 8;
 }
 
+size_t cdtw_pair_workspace_bytes(int64_t n, int L, int W, int flags, int with_path) {
+    if (n <= 0 || L < 1 || L > CDTW_MAX_QUERY || W < 0) return 0;
+    W = std::min(W, L - 1);
+    if (W > CDTW_PAIR_MAX_BAND) return 0;
+    Carver c;
+    if (flags & CDTW_PAIR_ZNORM) {
+        c.take<float>((size_t)n * L);
+        c.take<float>((size_t)n * L);
+    }
+    if (with_path) c.take<uint32_t>((size_t)n * pair_dirs_words(L, W));
+    return c.off;
+}
+
 static int pair_check(cdtw_handle h, const float* q, const float* s, int64_t n, int L,
                       int metric, int flags) {
     if (!q || !s || n < 0 || L < 1 || L > CDTW_MAX_QUERY)

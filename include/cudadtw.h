@@ -236,6 +236,12 @@ int cdtw_all_windows_noalloc(const float* d_query, int M, const float* d_subject
  * column runs (2 x L 32-bit words).  8-byte aligned device memory. */
 size_t cdtw_pair_path_bytes(int64_t n, int L);
 
+/* Device work memory cdtw_pair_fwd takes from the handle's grow-only workspace
+ * for n pairs: z-normalised copies of both series (flags & CDTW_PAIR_ZNORM)
+ * and, when a path is recorded (with_path != 0), 2 bits per band cell of
+ * predecessor choices, padded to the lane layout.  0 for invalid sizes. */
+size_t cdtw_pair_workspace_bytes(int64_t n, int L, int W, int flags, int with_path);
+
 /* Banded cDTW of n pairs (d_q[p], d_s[p]), each L float32 samples, row-major
  * n x L on the device: d_D[p] = minimum over warping paths with |i-j| <= W of
  * the summed cell cost (squared difference for CDTW_EUCLIDEAN, absolute for
