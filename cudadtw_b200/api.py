@@ -199,6 +199,17 @@ class Handle:
         self.M, self.W = q.size, min(W, q.size - 1)
         return loc.value, dist.value
 
+    def topk(self, subject, avg, std, k: int, metric=EUCLIDEAN):
+        """The k best non-overlapping windows of the query: (locations,
+        distances) best first, distances as the search prints them."""
+        locs = np.empty(k, np.int64)
+        dists = np.empty(k, np.float32)
+        found = ctypes.c_int()
+        self._check(self._lib.cdtw_topk(self._h, _ptr(subject), subject.numel(), _ptr(avg),
+                                        _ptr(std), _metric(metric), int(k), _ptr(locs),
+                                        _ptr(dists), ctypes.byref(found)))
+        return locs[:found.value], dists[:found.value]
+
     def search_counts(self):
         """(windows, below bsf after LB_Kim, reaching cDTW) of the last search."""
         c = (ctypes.c_int64 * 3)()

@@ -330,6 +330,35 @@ int cdtw_prune_cdtw(cdtw_handle h, const float* d_subject, int64_t N, const doub
     return finish_search(h, key, ctr, N - M + 1, metric == CDTW_EUCLIDEAN, location, distance);
 }
 
+int cdtw_topk(cdtw_handle h, const float* d_subject, int64_t N, const double* d_avg,
+              const float* d_std, int metric, int k, int64_t* locations, float* distances,
+              int* found) {
+    if (!h) return CDTW_EINVAL;
+    if (found) *found = 0;
+    if (!h->has_query) return set_error(h, CDTW_EINVAL, "no query set (cdtw_set_query)");
+    const int M = h->q.M;
+    if (!d_subject || !d_avg || !d_std || !locations || k < 1)
+        return set_error(h, CDTW_EINVAL, "bad top-k arguments");
+    if (N < M || N - M + 1 > (int64_t)INT32_MAX)
+        return set_error(h, CDTW_EINVAL, "subject length %lld for M=%d", (long long)N, M);
+    if (M < 11) return set_error(h, CDTW_EUNSUPPORTED, "top-k search needs M >= 11");
+    if (!valid_metric(metric)) return set_error(h, CDTW_EINVAL, "bad metric %d", metric);
+    CDTW_CUDA(h, cudaSetDevice(h->device));
+    CDTW_TRY(ensure_workspace(h, topk_workspace_bytes(N, M)));
+    std::vector<unsigned long long> picks;
+    CDTW_TRY(run_topk(h, d_subject, N, d_avg, d_std, metric == CDTW_EUCLIDEAN, k,
+                      (char*)h->ws, &picks));
+    for (size_t i = 0; i < picks.size(); ++i) {
+        const uint32_t bits = (uint32_t)(picks[i] >> 32);
+        float d;
+        memcpy(&d, &bits, 4);
+        locations[i] = (int64_t)(uint32_t)picks[i];
+        if (distances) distances[i] = metric == CDTW_EUCLIDEAN ? sqrtf(d) : d;
+    }
+    if (found) *found = (int)picks.size();
+    return CDTW_OK;
+}
+
 int cdtw_search_host(cdtw_handle h, const float* h_query, int M, const float* h_subject,
                      int64_t N, int W, int metric, int64_t* location, float* distance) {
     if (!h) return CDTW_EINVAL;

@@ -8,6 +8,8 @@
 #include <math.h>
 #include <string.h>
 
+#include <vector>
+
 #include "../../include/cudadtw.h"
 
 #define CDTW_INF __int_as_float(0x7f800000)
@@ -82,6 +84,10 @@ namespace cdtw {
 
 int set_error(cdtw_handle h, int status, const char* fmt, ...);
 void batch_plan_release(cdtw_handle h);
+// top-k non-overlapping matches (search.cu)
+size_t topk_workspace_bytes(int64_t N, int M);
+int run_topk(cdtw_handle h, const float* x, int64_t N, const double* mu, const float* sigma,
+             bool euclid, int k, char* ws_base, std::vector<unsigned long long>* picks);
 // pairwise cDTW forward / backward (pair.cu)
 void pair_shape(int L, int W, int* G, int* C);
 size_t pair_dirs_words(int L, int W);

@@ -23,6 +23,8 @@
 #include "common.cuh"
 
 #include <algorithm>
+#include <set>
+#include <vector>
 
 namespace cdtw {
 
@@ -150,7 +152,168 @@ size_t carve_search(int64_t N, int64_t Nw, SearchWs* ws, char* base) {
     return off;
 }
 
+// ---- top-k non-overlapping matches ------------------------------------------
+
+// One seed per segment s: the smallest-LB_Kim window start in [2Ms, 2Ms + M).
+// Seeds of different segments start at least M + 1 apart, so they never
+// overlap.  One warp per segment.
+__global__ void topk_seed_kernel(const float* __restrict__ lbkim, int Nw, int M, int nseg,
+                                 int32_t* __restrict__ sidx) {
+    const int lane = threadIdx.x & 31;
+    const int s = (int)(((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    if (s >= nseg) return;
+    const int lo = 2 * M * s, hi = min(lo + M, Nw);
+    unsigned long long best = ~0ull;
+    for (int w = lo + lane; w < hi; w += 32) best = min(best, pack_key(lbkim[w], (uint32_t)w));
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) best = min(best, __shfl_xor_sync(0xffffffffu, best, o));
+    if (lane == 0) sidx[s] = best == ~0ull ? lo : (int32_t)(uint32_t)best;
+}
+
+__global__ void cands_to_idx_kernel(const Cand* __restrict__ c, int n, int32_t* __restrict__ idx) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) idx[i] = c[i].w;
+}
+
+// Windows whose cDTW is at most T, as packed (distance, window) keys.
+__global__ void collect_kernel(const float* __restrict__ d, const int32_t* __restrict__ idx,
+                               int n, float T, unsigned long long* __restrict__ hits,
+                               int* __restrict__ nh, int cap) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n || !(d[i] <= T)) return;
+    const int at = atomicAdd(nh, 1);
+    if (at < cap) hits[at] = pack_key(d[i], (uint32_t)idx[i]);
+}
+
+struct TopkWs {
+    int32_t* sidx;
+    float* sd;
+    int32_t* idx;
+    float* d;
+    unsigned long long* hits;
+    int* nh;
+};
+
+size_t carve_topk(int64_t N, int64_t Nw, int M, int64_t cap, SearchWs* sw, TopkWs* tw,
+                  char* base) {
+    size_t off = carve_search(N, Nw, sw, base);
+    auto take = [&](size_t bytes) {
+        const size_t o = off;
+        off = (size_t)round_up((int64_t)(off + bytes), 256);
+        return base ? base + o : nullptr;
+    };
+    const int64_t nseg = div_up(Nw, 2 * (int64_t)M);
+    tw->sidx = (int32_t*)take(sizeof(int32_t) * nseg);
+    tw->sd = (float*)take(sizeof(float) * nseg);
+    tw->idx = (int32_t*)take(sizeof(int32_t) * Nw);
+    tw->d = (float*)take(sizeof(float) * Nw);
+    tw->hits = (unsigned long long*)take(sizeof(unsigned long long) * cap);
+    tw->nh = (int*)take(sizeof(int) * 2);
+    return off;
+}
+
+int64_t topk_cap(int64_t Nw) { return std::min<int64_t>(Nw, (int64_t)1 << 24); }
+
 }  // namespace
+
+size_t topk_workspace_bytes(int64_t N, int M) {
+    SearchWs sw;
+    TopkWs tw;
+    const int64_t Nw = N - M + 1;
+    return carve_topk(N, Nw, M, topk_cap(Nw), &sw, &tw, nullptr);
+}
+
+// Top-k non-overlapping matches of the handle's query.  Greedy selection in
+// (distance, window) order with windows overlapping an accepted one skipped.
+// The candidate threshold T is the 2k-th smallest cDTW among the segment
+// seeds: they are pairwise non-overlapping, and each accepted match overlaps
+// at most two of them, so every one of the first k greedy picks has a
+// distance <= T and all windows above T can be pruned.  Host-synchronous.
+int run_topk(cdtw_handle h, const float* x, int64_t N, const double* mu, const float* sigma,
+             bool euclid, int k, char* ws_base, std::vector<unsigned long long>* picks) {
+    const QueryPack& q = h->q;
+    const int M = q.M;
+    const int64_t Nw = N - M + 1;
+    SearchWs ws;
+    TopkWs tw;
+    const int64_t cap = topk_cap(Nw);
+    carve_topk(N, Nw, M, cap, &ws, &tw, ws_base);
+    const int nseg = (int)div_up(Nw, 2 * (int64_t)M);
+    // 1. LB_Kim of every window, seeds per segment, their exact cDTW
+    CDTW_TRY(launch_lb_kim(h, x, N, mu, sigma, nullptr, Nw, euclid, ws.lbkim, ws.seeds));
+    topk_seed_kernel<<<(unsigned)div_up((int64_t)nseg * 32, 256), 256, 0, h->stream>>>(
+        ws.lbkim, (int)Nw, M, nseg, tw.sidx);
+    CDTW_LAUNCH(h, "topk_seed_kernel");
+    CDTW_TRY(launch_cdtw_windows(h, x, N, mu, sigma, tw.sidx, nseg, euclid, tw.sd));
+    std::vector<float> sd(nseg);
+    CDTW_CUDA(h, cudaMemcpyAsync(sd.data(), tw.sd, sizeof(float) * nseg, cudaMemcpyDeviceToHost,
+                                 h->stream));
+    CDTW_CUDA(h, cudaStreamSynchronize(h->stream));
+    float T = INFINITY;
+    if ((int64_t)nseg >= 2 * (int64_t)k) {
+        std::nth_element(sd.begin(), sd.begin() + (2 * k - 1), sd.end());
+        T = sd[2 * k - 1];
+    }
+    // 2. bounds against T (the key holds T as the best-so-far)
+    const unsigned long long tkey = pack_key(T, 0xffffffffu);
+    CDTW_CUDA(h, cudaMemsetAsync(ws.ctr, 0, sizeof(int) * 8, h->stream));
+    CDTW_CUDA(h, cudaMemsetAsync(tw.nh, 0, sizeof(int) * 2, h->stream));
+    CDTW_CUDA(h, cudaMemcpyAsync(ws.key, &tkey, sizeof(tkey), cudaMemcpyHostToDevice, h->stream));
+    const int grid = h->sm_count * 8;
+    compact_kim_kernel<<<grid, 256, 0, h->stream>>>(ws.lbkim, (int)Nw, ws.key, ws.q1, ws.ctr + 0);
+    CDTW_LAUNCH(h, "compact_kim_kernel");
+    CDTW_TRY(launch_stream_envelope(h, x, N, q.W, ws.envscratch, ws.xenv));
+    if (euclid)
+        keogh_filter_kernel<true><<<grid, 256, 0, h->stream>>>(
+            x, mu, sigma, q.zq, q.env, ws.xenv, ws.lbkim, M, ws.q1, ws.ctr + 0, ws.key, ws.q2,
+            ws.ctr + 1);
+    else
+        keogh_filter_kernel<false><<<grid, 256, 0, h->stream>>>(
+            x, mu, sigma, q.zq, q.env, ws.xenv, ws.lbkim, M, ws.q1, ws.ctr + 0, ws.key, ws.q2,
+            ws.ctr + 1);
+    CDTW_LAUNCH(h, "keogh_filter_kernel");
+    int cnt[2];
+    CDTW_CUDA(h, cudaMemcpyAsync(cnt, ws.ctr, sizeof(cnt), cudaMemcpyDeviceToHost, h->stream));
+    CDTW_CUDA(h, cudaStreamSynchronize(h->stream));
+    h->last_counts[0] = Nw;
+    h->last_counts[1] = cnt[0];
+    h->last_counts[2] = cnt[1];
+    // 3. exact cDTW of the survivors, those <= T collected
+    const int ns = cnt[1];
+    if (ns > 0) {
+        cands_to_idx_kernel<<<(unsigned)div_up(ns, 256), 256, 0, h->stream>>>(ws.q2, ns, tw.idx);
+        CDTW_LAUNCH(h, "cands_to_idx_kernel");
+        CDTW_TRY(launch_cdtw_windows(h, x, N, mu, sigma, tw.idx, ns, euclid, tw.d));
+        collect_kernel<<<(unsigned)div_up(ns, 256), 256, 0, h->stream>>>(tw.d, tw.idx, ns, T,
+                                                                        tw.hits, tw.nh, (int)cap);
+        CDTW_LAUNCH(h, "collect_kernel");
+    }
+    int nh = 0;
+    CDTW_CUDA(h, cudaMemcpyAsync(&nh, tw.nh, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    CDTW_CUDA(h, cudaStreamSynchronize(h->stream));
+    if (nh > cap)
+        return set_error(h, CDTW_EUNSUPPORTED, "%d windows under the top-k threshold (limit %lld)",
+                         nh, (long long)cap);
+    std::vector<unsigned long long> hits(nh);
+    if (nh > 0) {
+        CDTW_CUDA(h, cudaMemcpyAsync(hits.data(), tw.hits, sizeof(unsigned long long) * nh,
+                                     cudaMemcpyDeviceToHost, h->stream));
+        CDTW_CUDA(h, cudaStreamSynchronize(h->stream));
+    }
+    // 4. greedy non-overlapping selection, lowest (distance, window) first
+    std::sort(hits.begin(), hits.end());
+    std::set<int64_t> taken;
+    picks->clear();
+    for (const unsigned long long key : hits) {
+        if ((int)picks->size() >= k) break;
+        const int64_t w = (int64_t)(uint32_t)key;
+        auto it = taken.lower_bound(w - M + 1);
+        if (it != taken.end() && *it < w + M) continue;  // overlaps an accepted window
+        taken.insert(w);
+        picks->push_back(key);
+    }
+    return CDTW_OK;
+}
 
 size_t search_workspace_bytes(int64_t N, int M) {
     SearchWs ws;

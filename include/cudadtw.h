@@ -129,6 +129,19 @@ int cdtw_lb_keogh(cdtw_handle h, const float* d_subject, int64_t N, const double
 int cdtw_prune_cdtw(cdtw_handle h, const float* d_subject, int64_t N, const double* d_avg,
                     const float* d_std, int metric, int64_t* location, float* distance);
 
+/* The k best pairwise non-overlapping windows of the handle's query: greedy
+ * selection in (distance, window) order, a window overlapping (start within
+ * M - 1 of) an accepted one is skipped.  locations[0..*found) / distances as
+ * cdtw_prune_cdtw prints them, best first; *found < k only when the subject
+ * holds fewer non-overlapping windows.  No reference counterpart (the
+ * reference reports the single best match; UCR keeps one best-so-far).
+ * Pruned like the search: LB_Kim, LB_Keogh and reverse LB_Keogh against a
+ * threshold that provably bounds the k-th match (the 2k-th smallest cDTW of
+ * pairwise non-overlapping seed windows).  Host-synchronous; needs M >= 11. */
+int cdtw_topk(cdtw_handle h, const float* d_subject, int64_t N, const double* d_avg,
+              const float* d_std, int metric, int k, int64_t* locations, float* distances,
+              int* found);
+
 /* The whole GPU-DTW search from host buffers (GPU-dtw.cu:59-90): H2D of the
  * subject and query, z-normalisation, statistics, pruned search. */
 int cdtw_search_host(cdtw_handle h, const float* h_query, int M, const float* h_subject,
