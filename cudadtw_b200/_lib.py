@@ -46,6 +46,8 @@ SIGNATURES = {
     "cdtw_all_windows_noalloc": (c_int, [c_vp, c_int, c_vp, c_i64, c_int, c_int, c_vp, c_vp,
                                          ctypes.c_char_p, c_int]),
     "cdtw_pair_path_bytes": (ctypes.c_size_t, [c_i64, c_int]),
+    "cdtw_refine_templates": (c_int, [c_vp, c_vp, c_i64, c_vp, c_vp, c_vp, c_int, c_vp, c_int,
+                                      c_int, ctypes.c_float, c_int, c_vp]),
     "cdtw_pair_workspace_bytes": (ctypes.c_size_t, [c_i64, c_int, c_int, c_int, c_int]),
     "cdtw_pair_fwd": (c_int, [c_vp, c_vp, c_vp, c_i64, c_int, c_int, c_int, c_int, c_vp, c_vp]),
     "cdtw_pair_bwd": (c_int, [c_vp, c_vp, c_vp, c_i64, c_int, c_int, c_int, c_vp, c_vp, c_vp,

@@ -329,3 +329,30 @@ class Handle:
             self._h, _ptr(q), _ptr(s), n, L, _metric(metric), self.PAIR_ZNORM if znorm else 0,
             _ptr(path), _ptr(dD), _ptr(dq if need_q else None), _ptr(ds if need_s else None)))
         return (dq if need_q else None), (ds if need_s else None)
+
+    # -- template refinement ----------------------------------------------------
+    def refine_templates(self, subject: torch.Tensor, templates, bands, locations, steps: int,
+                         lr: float = 1e-2, metric=EUCLIDEAN):
+        """Adam refinement of templates against their matched windows
+        (cdtw_refine_templates).  ``templates``: list of 1-D arrays; ``bands``:
+        W per template; ``locations``: (nt, k) window starts.  Returns the
+        refined templates (list of float32 arrays) and the (steps+1, nt) losses."""
+        _dev(subject, torch.float32, "subject")
+        ts = [np.ascontiguousarray(t, dtype=np.float32) for t in templates]
+        nt = len(ts)
+        flat = torch.from_numpy(np.concatenate(ts)).to(subject.device)
+        ms = np.array([t.size for t in ts], dtype=np.int32)
+        ws = np.ascontiguousarray(bands, dtype=np.int32)
+        loc = np.ascontiguousarray(locations, dtype=np.int64)
+        if loc.ndim != 2 or loc.shape[0] != nt:
+            raise ValueError("locations must be (n_templates, k)")
+        losses = np.empty((steps + 1, nt), np.float32)
+        self._check(self._lib.cdtw_refine_templates(
+            self._h, _ptr(subject), subject.numel(), _ptr(flat), _ptr(ms), _ptr(ws), nt,
+            _ptr(loc), loc.shape[1], int(steps), float(lr), _metric(metric), _ptr(losses)))
+        out = flat.cpu().numpy()
+        res, o = [], 0
+        for m in ms:
+            res.append(out[o:o + m].copy())
+            o += m
+        return res, losses

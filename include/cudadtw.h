@@ -276,6 +276,25 @@ int cdtw_pair_bwd(cdtw_handle h, const float* d_q, const float* d_s, int64_t n, 
                   int metric, int flags, const void* d_path, const float* d_dD, float* d_dq,
                   float* d_ds);
 
+/* ---- template refinement ---------------------------------------------------------- */
+
+/* Adam refinement of nt query templates against their matched windows (no
+ * reference counterpart).  d_templates: the templates' raw float32 values
+ * concatenated (sum of Ms floats, device), updated in place.  Template t
+ * (length Ms[t], band Ws[t] <= CDTW_PAIR_MAX_BAND) is fitted to the k windows
+ * of d_subject starting at locations[t*k .. t*k+k) (host array, e.g. from
+ * cdtw_topk): loss_t = mean over its windows of the banded cDTW between the
+ * z-normalised template and the z-normalised window (cdtw_pair_fwd with
+ * CDTW_PAIR_ZNORM); each step takes the gradient through cdtw_pair_bwd and
+ * applies Adam (learning rate lr, beta1 0.9, beta2 0.999, eps 1e-8) to the raw
+ * template values.  All `steps` steps run as one CUDA graph.  losses (host,
+ * may be NULL) receives (steps + 1) x nt values: row s = the losses before
+ * step s, row `steps` = after the last step.  Host-synchronous; allocates its
+ * working memory for the call. */
+int cdtw_refine_templates(cdtw_handle h, const float* d_subject, int64_t N, float* d_templates,
+                          const int* Ms, const int* Ws, int nt, const int64_t* locations, int k,
+                          int steps, float lr, int metric, float* losses);
+
 /* ---- kernel selection ----------------------------------------------------------- */
 
 enum cdtw_variant {
