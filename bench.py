@@ -474,6 +474,61 @@ def refine_subresult(h, dev) -> dict:
             "fp64_recheck_max_rel": float(max(check))}
 
 
+def profile_case(name: str) -> None:
+    """One small run of a scope row (twice, untimed) for an ncu capture:
+    search = config-1 pruned search (2^25 metal-like, M=512, P=10); topk =
+    top-1000 of one M=256 template on a 2^22 ECG-like stream; pair = 256 pairs
+    of L=2048, W=409 and 4096 pairs of L=256, W=25 (forward, forward with path,
+    backward); refine = 8 templates x 200 matches, 5 Adam steps."""
+    import torch
+    from cudadtw_b200 import Handle, synth
+    dev = torch.device("cuda", 0)
+    with Handle(0) as h:
+        for _ in range(2):
+            if name == "search":
+                x = synth.metal_like(1 << 25, seed=1)
+                dx = torch.from_numpy(x).to(dev)
+                q, _ = synth.cut_query(x, 512, seed=622, noise=0.1)
+                avg, std = h.avg_std(dx, 512)
+                h.set_query(q, synth.band_from_percent(512, 10))
+                h.prune_cdtw(dx, avg, std)
+            elif name == "topk":
+                x = synth.ecg_like(1 << 22, seed=0)
+                dx = torch.from_numpy(x).to(dev)
+                q, _ = synth.cut_query(x, 256, seed=5, noise=0.2)
+                avg, std = h.avg_std(dx, 256)
+                h.set_query(q, 25)
+                h.topk(dx, avg, std, 1000)
+            elif name == "pair":
+                for n, L, W in ((256, 2048, 409), (4096, 256, 25)):
+                    rng = np.random.default_rng(0)
+                    q = torch.from_numpy(np.cumsum(rng.standard_normal((n, L)), 1)
+                                         .astype(np.float32)).to(dev)
+                    s = torch.from_numpy(np.cumsum(rng.standard_normal((n, L)), 1)
+                                         .astype(np.float32)).to(dev)
+                    path = torch.empty(h.pair_path_bytes(n, L), dtype=torch.uint8, device=dev)
+                    h.pair_fwd(q, s, W)
+                    h.pair_fwd(q, s, W, path=path)
+                    h.pair_bwd(q, s, path)
+            elif name == "refine":
+                x = synth.ecg_like(1 << 20, seed=0)
+                dx = torch.from_numpy(x).to(dev)
+                temps, bands, locs = [], [], []
+                for i in range(8):
+                    m = 128 + 32 * i
+                    q, _ = synth.cut_query(x, m, seed=40 + i, noise=0.2)
+                    avg, std = h.avg_std(dx, m)
+                    h.set_query(q, m // 10)
+                    locs.append(h.topk(dx, avg, std, 200)[0][:200])
+                    temps.append(q)
+                    bands.append(m // 10)
+                h.refine_templates(dx, temps, bands, np.stack(locs), steps=5)
+            else:
+                raise SystemExit(f"unknown profile case {name}")
+            torch.cuda.synchronize()
+    print("profile case done:", name)
+
+
 def ctypes_peak(lib, h) -> float:
     import ctypes
     v = ctypes.c_double()
@@ -489,12 +544,17 @@ def main() -> None:
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--profile", choices=["search", "topk", "pair", "refine"],
+                    help="run one small case of that row twice (for ncu) and exit")
     ap.add_argument("--no-sub", action="store_true",
                     help="skip the pruned / batched search and pair fwd/bwd sub-results")
     ap.add_argument("--only-kernels", action="store_true",
                     help="device-timed steps only (no calibration, e2e or CPU baseline): "
                          "the target of ncu captures")
     args = ap.parse_args()
+    if args.profile:
+        profile_case(args.profile)
+        return
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))

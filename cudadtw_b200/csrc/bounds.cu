@@ -17,6 +17,8 @@
 //     uniform, read once per step for all lanes).
 #include "common.cuh"
 
+#include <algorithm>
+
 namespace cdtw {
 
 namespace {
@@ -64,66 +66,56 @@ lb_kim_kernel(const float* __restrict__ x, const double* __restrict__ mu,
     }
 }
 
-// van Herk / Gil-Werman, pass 1: prefix and suffix min/max inside segments
-// of K = 2W+1 samples (one thread per segment).
-__global__ void __launch_bounds__(128)
-env_segments_kernel(const float* __restrict__ x, int64_t N, int K, float* __restrict__ pmin,
-                    float* __restrict__ pmax, float* __restrict__ smin, float* __restrict__ smax) {
-    const int64_t seg = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const int64_t a = seg * K;
-    if (a >= N) return;
-    const int64_t b = min(a + K, N);
-    float lo = CDTW_INF, hi = -CDTW_INF;
-    for (int64_t i = a; i < b; ++i) {
-        const float v = x[i];
-        lo = fminf(lo, v);
-        hi = fmaxf(hi, v);
-        pmin[i] = lo;
-        pmax[i] = hi;
-    }
-    lo = CDTW_INF;
-    hi = -CDTW_INF;
-    for (int64_t i = b - 1; i >= a; --i) {
-        const float v = x[i];
-        lo = fminf(lo, v);
-        hi = fmaxf(hi, v);
-        smin[i] = lo;
-        smax[i] = hi;
-    }
-}
+// Stream envelope of the reverse LB_Keogh (the data envelope of
+// UCR_DTW_BIN.cpp:607): env[p] = (min, max) of x over [p-W, p+W] clipped to
+// the stream.  One block per tile of T outputs: the tile and its 2W halo are
+// staged in shared memory (+inf / -inf outside the stream, which leaves the
+// extrema of clipped windows unchanged); spans of 2^j samples are doubled in
+// place up to the largest power of two p <= K = 2W+1, and output t takes the
+// spans starting at t and at t + K - p.  Coalesced in and out, no scratch.
+constexpr int kEnvThreads = 512;
+constexpr int kEnvSmemFloats = 50176;  // both arrays: 196 KB
 
-// pass 2: extrema over [p-W, p+W] clipped to the stream.  A full window of
-// K samples either starts a segment (prefix extremum at its end) or spans two
-// segments (suffix extremum at its start combined with the prefix extremum
-// at its end); windows clipped at the stream ends are handled the same way.
-__global__ void __launch_bounds__(256)
-env_combine_kernel(const float* __restrict__ x, int64_t N, int W, const float* __restrict__ pmin,
-                   const float* __restrict__ pmax, const float* __restrict__ smin,
-                   const float* __restrict__ smax, float2* __restrict__ env) {
-    const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= N) return;
-    const int64_t K = 2 * (int64_t)W + 1;
-    const int64_t a = max((int64_t)0, p - W), b = min(N - 1, p + W);
-    const int64_t sa = a / K, sb = b / K;
-    float lo, hi;
-    if (sa != sb) {
-        lo = fminf(smin[a], pmin[b]);
-        hi = fmaxf(smax[a], pmax[b]);
-    } else if (a == sa * K) {  // window starts its segment
-        lo = pmin[b];
-        hi = pmax[b];
-    } else if (b == min(N, (sa + 1) * K) - 1) {  // window ends its segment
-        lo = smin[a];
-        hi = smax[a];
-    } else {  // clipped on both sides (stream shorter than the band): direct
-        lo = CDTW_INF;
-        hi = -CDTW_INF;
-        for (int64_t i = a; i <= b; ++i) {
-            lo = fminf(lo, x[i]);
-            hi = fmaxf(hi, x[i]);
+__global__ void __launch_bounds__(kEnvThreads)
+env_window_kernel(const float* __restrict__ x, int64_t N, int W, int T, float2* __restrict__ env) {
+    extern __shared__ float esm[];
+    const int K = 2 * W + 1;
+    const int S = T + 2 * W;
+    float* lo = esm;
+    float* hi = esm + S;
+    const int64_t t0 = (int64_t)blockIdx.x * T;
+    for (int i = threadIdx.x; i < S; i += kEnvThreads) {
+        const int64_t g = t0 - W + i;
+        const bool in = g >= 0 && g < N;
+        const float v = in ? __ldg(x + g) : 0.f;
+        lo[i] = in ? v : CDTW_INF;
+        hi[i] = in ? v : -CDTW_INF;
+    }
+    __syncthreads();
+    int p = 1;
+    for (; 2 * p <= K; p *= 2) {
+        // entry i becomes the extremum of [i, i + 2p); chunks in increasing i,
+        // so a partner i + p > i is never one this pass already rewrote
+        for (int i0 = 0; i0 < S - p; i0 += kEnvThreads) {
+            const int i = i0 + threadIdx.x;
+            float a = 0.f, b = 0.f;
+            if (i < S - p) {
+                a = fminf(lo[i], lo[i + p]);
+                b = fmaxf(hi[i], hi[i + p]);
+            }
+            __syncthreads();
+            if (i < S - p) {
+                lo[i] = a;
+                hi[i] = b;
+            }
+            __syncthreads();
         }
     }
-    env[p] = make_float2(lo, hi);
+    for (int t = threadIdx.x; t < T; t += kEnvThreads) {
+        if (t0 + t >= N) break;
+        const int c = t + K - p;
+        env[t0 + t] = make_float2(fminf(lo[t], lo[c]), fmaxf(hi[t], hi[c]));
+    }
 }
 
 // Forward LB_Keogh (window vs query envelope, bounds.cuh:128-140) and reverse
@@ -183,22 +175,20 @@ int launch_lb_kim(cdtw_handle h, const float* x, int64_t N, const double* mu, co
     return CDTW_OK;
 }
 
-size_t stream_envelope_scratch_bytes(int64_t N) { return (size_t)N * 4 * sizeof(float); }
+size_t stream_envelope_scratch_bytes(int64_t) { return 0; }
 
-int launch_stream_envelope(cdtw_handle h, const float* x, int64_t N, int W, float* scratch,
+int launch_stream_envelope(cdtw_handle h, const float* x, int64_t N, int W, float*,
                            float2* env) {
-    const int K = 2 * W + 1;
-    float* pmin = scratch;
-    float* pmax = scratch + N;
-    float* smin = scratch + 2 * N;
-    float* smax = scratch + 3 * N;
-    const int64_t segs = div_up(N, K);
-    env_segments_kernel<<<(unsigned)div_up(segs, 128), 128, 0, h->stream>>>(x, N, K, pmin, pmax,
-                                                                          smin, smax);
-    CDTW_LAUNCH(h, "env_segments_kernel");
-    env_combine_kernel<<<(unsigned)div_up(N, 256), 256, 0, h->stream>>>(x, N, W, pmin, pmax,
-                                                                      smin, smax, env);
-    CDTW_LAUNCH(h, "env_combine_kernel");
+    // tile: at least 2048 outputs (or 2W when the halo is larger), within the
+    // shared-memory budget of both arrays
+    const int T = std::max(1, std::min(std::max(2048, 2 * W), kEnvSmemFloats / 2 - 2 * W));
+    if (kEnvSmemFloats / 2 - 2 * W < 1)
+        return set_error(h, CDTW_EUNSUPPORTED, "band W=%d too wide for the stream envelope", W);
+    const size_t smem = (size_t)2 * (T + 2 * W) * sizeof(float);
+    CDTW_CUDA(h, cudaFuncSetAttribute((const void*)env_window_kernel,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    env_window_kernel<<<(unsigned)div_up(N, T), kEnvThreads, smem, h->stream>>>(x, N, W, T, env);
+    CDTW_LAUNCH(h, "env_window_kernel");
     return CDTW_OK;
 }
 

@@ -17,6 +17,7 @@ namespace {
 constexpr int kStatsRounds = 64;                 // rounds of 32 windows per warp
 constexpr int kStatsWarpWindows = 32 * kStatsRounds;
 constexpr int kStatsBlock = 128;                 // 4 warps per block
+constexpr int kStatsBatch = 8;                   // rounds whose samples load together
 
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll
@@ -53,27 +54,41 @@ avg_std_kernel(const XT* __restrict__ x, int64_t N, int M, double* __restrict__ 
     s1 = warp_sum(s1);
     s2 = warp_sum(s2);
     const double invM = 1.0 / (double)M;
-    for (int r = 0; r < kStatsRounds; ++r) {
-        const int64_t w = a + (int64_t)r * 32 + lane;
-        if (a + (int64_t)r * 32 >= Nw) break;  // warp-uniform
-        double d1 = 0.0, d2 = 0.0;
-        if (w < Nw - 1) {
-            // window w+1 = window w + x[w+M] - x[w]
-            const double vin = (double)x[w + M] - c, vout = (double)x[w] - c;
-            d1 = vin - vout;
-            d2 = vin * vin - vout * vout;
+    // the entering / leaving samples of kStatsBatch rounds are loaded together
+    // (one memory latency per batch instead of one per round)
+    for (int r0 = 0; r0 < kStatsRounds; r0 += kStatsBatch) {
+        if (a + (int64_t)r0 * 32 >= Nw) break;  // warp-uniform
+        XT xin[kStatsBatch], xout[kStatsBatch];
+#pragma unroll
+        for (int u = 0; u < kStatsBatch; ++u) {
+            const int64_t w = a + (int64_t)(r0 + u) * 32 + lane;
+            const bool ok = w < Nw - 1;
+            xin[u] = ok ? x[w + M] : (XT)0;
+            xout[u] = ok ? x[w] : (XT)0;
         }
-        const double i1 = warp_incl_scan(d1, lane), i2 = warp_incl_scan(d2, lane);
-        // sums of window w: base + exclusive scan
-        const double w1 = s1 + (i1 - d1), w2 = s2 + (i2 - d2);
-        if (w < Nw) {
-            const double m1 = w1 * invM;
-            const double var = w2 * invM - m1 * m1;
-            mu[w] = c + m1;
-            sigma[w] = var > 0.0 ? (ST)sqrt(var) : (ST)1;
+#pragma unroll
+        for (int u = 0; u < kStatsBatch; ++u) {
+            const int64_t w = a + (int64_t)(r0 + u) * 32 + lane;
+            if (a + (int64_t)(r0 + u) * 32 >= Nw) break;  // warp-uniform
+            double d1 = 0.0, d2 = 0.0;
+            if (w < Nw - 1) {
+                // window w+1 = window w + x[w+M] - x[w]
+                const double vin = (double)xin[u] - c, vout = (double)xout[u] - c;
+                d1 = vin - vout;
+                d2 = vin * vin - vout * vout;
+            }
+            const double i1 = warp_incl_scan(d1, lane), i2 = warp_incl_scan(d2, lane);
+            // sums of window w: base + exclusive scan
+            const double w1 = s1 + (i1 - d1), w2 = s2 + (i2 - d2);
+            if (w < Nw) {
+                const double m1 = w1 * invM;
+                const double var = w2 * invM - m1 * m1;
+                mu[w] = c + m1;
+                sigma[w] = var > 0.0 ? (ST)sqrt(var) : (ST)1;
+            }
+            s1 += __shfl_sync(0xffffffffu, i1, 31);
+            s2 += __shfl_sync(0xffffffffu, i2, 31);
         }
-        s1 += __shfl_sync(0xffffffffu, i1, 31);
-        s2 += __shfl_sync(0xffffffffu, i2, 31);
     }
 }
 
