@@ -26,12 +26,14 @@ peak_cell_kernel(const float* __restrict__ seed, int iters, float* __restrict__ 
     for (int it = 0; it < iters; ++it) {
 #pragma unroll
         for (int c = 0; c < kChains; ++c) {
-            // two cells per chain per iteration, each FADD + FMNMX3 + FFMA
+            // two independent cells per chain per iteration, each FADD + FMNMX3
+            // + FFMA (independent within the iteration: the highest issue rate
+            // of the update, the strictest denominator)
             const float d0 = z - a[c];
             const float m0 = min3f(a[c], b[c], q);
             const float v0 = fmaf(d0, d0, m0);
             const float d1 = q - b[c];
-            const float m1 = min3f(v0, b[c], a[c]);
+            const float m1 = min3f(b[c], a[c], z);
             const float v1 = fmaf(d1, d1, m1);
             a[c] = v0;  // values may grow to +inf; inf arithmetic issues at the same rate
             b[c] = v1;
