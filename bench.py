@@ -281,7 +281,7 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
                 "e2e": {"value": e2e, "unit": "GCUPS",
                         "h2d_bytes_per_step": len(bands) * (x.nbytes + q.nbytes),
                         "d2h_bytes_per_step": len(bands) * nw * 4},
-                "roofline": {"bound": "alu", "kernel": "cdtw_reg_kernel",
+                "roofline": {"bound": "alu", "kernel": "cdtw_reg2_kernel",
                              "achieved": ach, "peak": peak / 1e9, "unit": "GCUPS",
                              "frac": ach / (peak / 1e9), "traffic": None,
                              "per_band": {str(w): a for w, a in zip(bands, achieved)},

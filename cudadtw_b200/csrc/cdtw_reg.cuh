@@ -86,6 +86,84 @@ cdtw_reg_kernel(const float* __restrict__ x, const double* __restrict__ mu,
     out[t] = res;
 }
 
+// Two windows per thread: both read the same query band values at a row (the
+// band of row j is q[j-W .. j+W] whatever the window), so the shared-memory
+// query loads are paid once for 2(2W+1) cells, and the two windows' cell
+// chains interleave (two independent min chains per thread).  Listed windows
+// 2t and 2t+1; a missing second window computes a copy of the first and is
+// not stored.
+constexpr int kMaxReg2W = 48;
+
+template <int W, bool EU>
+__global__ void __launch_bounds__(kRegBlock, 1)
+cdtw_reg2_kernel(const float* __restrict__ x, const double* __restrict__ mu,
+                 const float* __restrict__ sigma, const float4* __restrict__ qpad4, int lq4,
+                 int M, int Nw, const int32_t* __restrict__ idx, int L, float* __restrict__ out) {
+    extern __shared__ float4 sq4[];
+    for (int e = threadIdx.x; e < 4 * lq4; e += blockDim.x) sq4[e] = qpad4[e];
+    __syncthreads();
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (2 * t >= L) return;
+    const int t1 = min(2 * t + 1, L - 1);
+    int w0 = idx ? idx[2 * t] : 2 * t;
+    int w1 = idx ? idx[t1] : t1;
+    const bool ok0 = w0 >= 0 && w0 < Nw, ok1 = w1 >= 0 && w1 < Nw;
+    if (!ok0) w0 = 0;  // a listed window outside the subject: NaN, no access
+    if (!ok1) w1 = 0;
+    const Norm n0 = make_norm(mu[w0], sigma[w0]);
+    const Norm n1 = make_norm(mu[w1], sigma[w1]);
+    const float* __restrict__ x0 = x + w0;
+    const float* __restrict__ x1 = x + w1;
+
+    constexpr int B = 2 * W + 1;
+    constexpr int NQ4 = (B + 3) / 4;
+    float p0[B + 1], p1[B + 1];
+#pragma unroll
+    for (int k = 0; k <= B; ++k) {
+        p0[k] = CDTW_INF;
+        p1[k] = CDTW_INF;
+    }
+    p0[W] = 0.0f;
+    p1[W] = 0.0f;
+    float r0 = CDTW_INF, r1 = CDTW_INF;
+
+    for (int j0 = 0; j0 < M; j0 += 4) {
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int j = j0 + u;
+            const int jc = min(j, M - 1);
+            const float z0 = znorm(n0, __ldg(x0 + jc));
+            const float z1 = znorm(n1, __ldg(x1 + jc));
+            const float4* qr = sq4 + u * lq4 + (j0 >> 2);
+            float qv[NQ4 * 4];
+#pragma unroll
+            for (int r = 0; r < NQ4; ++r) {
+                const float4 v = qr[r];
+                qv[4 * r + 0] = v.x;
+                qv[4 * r + 1] = v.y;
+                qv[4 * r + 2] = v.z;
+                qv[4 * r + 3] = v.w;
+            }
+            float l0 = CDTW_INF, l1 = CDTW_INF;
+#pragma unroll
+            for (int k = 0; k < B; ++k) {
+                const float m0 = min3f(p0[k], p0[k + 1], l0);
+                const float m1 = min3f(p1[k], p1[k + 1], l1);
+                l0 = cell<EU>(z0 - qv[k], m0);
+                l1 = cell<EU>(z1 - qv[k], m1);
+                p0[k] = l0;  // p[k] is not read again this row
+                p1[k] = l1;
+            }
+            if (j == M - 1) {
+                r0 = p0[W];
+                r1 = p1[W];
+            }
+        }
+    }
+    out[2 * t] = ok0 ? r0 : __int_as_float(0x7fc00000);
+    if (2 * t + 1 < L) out[2 * t + 1] = ok1 ? r1 : __int_as_float(0x7fc00000);
+}
+
 // cDTW of one window (xw, normalisation nm) against the query whose padded
 // copies sit in shared memory (sq4, lq4 float4 per copy) with its envelope
 // senv, abandoning once the last row minimum plus the remaining suffix of the
@@ -208,6 +286,17 @@ struct RegRange {
 
 }  // namespace
 
+template <int LO, int HI>
+struct Reg2Range {
+    static void fill(RegKernel* eu, RegKernel* mh) {
+        if constexpr (LO <= HI) {
+            eu[LO] = cdtw_reg2_kernel<LO, true>;
+            mh[LO] = cdtw_reg2_kernel<LO, false>;
+            Reg2Range<LO + 1, HI>::fill(eu, mh);
+        }
+    }
+};
+
 // Defined in cdtw_reg_part*.cu: each fills its range of bands.
 void reg_fill_part0(void** eu, void** mh, void** seu, void** smh);
 void reg_fill_part1(void** eu, void** mh, void** seu, void** smh);
@@ -215,5 +304,7 @@ void reg_fill_part2(void** eu, void** mh, void** seu, void** smh);
 void reg_fill_part3(void** eu, void** mh, void** seu, void** smh);
 void reg_fill_part4(void** eu, void** mh, void** seu, void** smh);
 void reg_fill_part5(void** eu, void** mh, void** seu, void** smh);
+void reg2_fill_part0(void** eu, void** mh);  // two-window kernels, cdtw_reg2_part*.cu
+void reg2_fill_part1(void** eu, void** mh);
 
 }  // namespace cdtw
