@@ -193,7 +193,7 @@ constexpr int kWalkStages = 4;            // direction chunks in flight during b
 constexpr int kMoveLog = kWalkRows * 16;  // bytes: the moves of one chunk (<= kWalkRows * S)
 
 template <int C, bool EU, bool DIRS>
-__global__ void __launch_bounds__(kPairThreads, DIRS ? 2 : 4) pair_fwd_kernel(const PairArgs a) {
+__global__ void __launch_bounds__(kPairThreads, 4) pair_fwd_kernel(const PairArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
     const int G = a.G, L = a.L, W = a.W;
     const int tid = threadIdx.x;
