@@ -405,8 +405,33 @@ __global__ void pair_znorm_kernel(const float* __restrict__ q, const float* __re
     }
 }
 
-// Exclusive FP64 prefix sums P[0..L] of the L floats in x, by one warp
-// (each lane a contiguous slice, then a scan of the slice totals).
+constexpr int kBwdThreads = 128;
+
+// Block-wide FP64 sums of a and b (every thread gets them); blocks of 1 to 4
+// warps; red holds 2 x 4 doubles.
+__device__ __forceinline__ void block_sum2(double& a, double& b, double* red) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        a += __shfl_xor_sync(kFull, a, o);
+        b += __shfl_xor_sync(kFull, b, o);
+    }
+    __syncthreads();  // red may still be read from a previous call
+    if (lane == 0) {
+        red[wid] = a;
+        red[4 + wid] = b;
+    }
+    __syncthreads();
+    const int nw = blockDim.x >> 5;
+    a = 0.0;
+    b = 0.0;
+    for (int w = 0; w < nw; ++w) {
+        a += red[w];
+        b += red[4 + w];
+    }
+}
+
+// The same by one warp (lane slices, warp scan of the slice totals).
 __device__ void warp_prefix(const float* x, double* P, int L, int lane) {
     const int per = (L + 31) / 32;
     const int lo = min(lane * per, L), hi = min(lo + per, L);
@@ -427,26 +452,62 @@ __device__ void warp_prefix(const float* x, double* P, int L, int lane) {
     __syncwarp();
 }
 
-// Backward: one warp per pair, the pair's z values staged in shared memory.
-// g_q[i] = sum over the row run [a_i, b_i] of f'(zq_i - zs_j), g_s[j] = -sum
-// over the column run; then through the z-normalisation and scaled by dD.
-// For the squared cost f'(d) = 2d and a run sum is 2 (len zq_i - (P[b+1] -
-// P[a])) with FP64 prefix sums P of the other series: no per-run loop, so
-// lanes with long runs do not hold up the warp.  Runs are clamped to
+// Exclusive FP64 prefix sums P[0..L] of the L floats in x by the block: each
+// thread a contiguous slice, a scan of the slice totals across the block.
+__device__ void block_prefix(const float* x, double* P, int L, double* red) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int nt = blockDim.x;
+    const int per = (L + nt - 1) / nt;
+    const int lo = min((int)threadIdx.x * per, L), hi = min(lo + per, L);
+    double tot = 0.0;
+    for (int t = lo; t < hi; ++t) tot += (double)x[t];
+    double inc = tot;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const double v = __shfl_up_sync(kFull, inc, o);
+        if (lane >= o) inc += v;
+    }
+    __syncthreads();
+    if (lane == 31) red[wid] = inc;
+    __syncthreads();
+    double base = 0.0;
+    for (int w = 0; w < wid; ++w) base += red[w];
+    double run = base + inc - tot;
+    for (int t = lo; t < hi; ++t) {
+        P[t] = run;
+        run += (double)x[t];
+    }
+    if ((int)threadIdx.x == nt - 1) P[L] = base + inc;
+    __syncthreads();
+}
+
+// Backward, one pair per scope: a warp (BLOCK = false, several pairs per
+// block, L <= 1024) or the whole block (BLOCK = true, four warps, longer
+// series); the pair's z values staged in shared memory.  g_q[i] = sum over the
+// row run [a_i, b_i] of f'(zq_i - zs_j), g_s[j] = -sum over the column run;
+// then through the z-normalisation and scaled by dD.  For the squared cost
+// f'(d) = 2d and a run sum is 2 (len zq_i - (P[b+1] - P[a])) with FP64 prefix
+// sums P of the other series: no per-run loop.  Runs are clamped to
 // [0, L-1], so a damaged path record cannot index outside the staged series.
-template <bool EU>
-__global__ void __launch_bounds__(128)
+template <bool EU, bool BLOCK>
+__global__ void __launch_bounds__(kBwdThreads)
 pair_bwd_kernel(const float* __restrict__ q, const float* __restrict__ s, int64_t n, int L,
                 const double* __restrict__ hdr, const uint32_t* __restrict__ rows,
                 const uint32_t* __restrict__ cols, const float* __restrict__ dD,
                 float* __restrict__ dq, float* __restrict__ ds) {
     extern __shared__ __align__(16) unsigned char bsm[];
-    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-    const int64_t pr = (int64_t)blockIdx.x * (blockDim.x >> 5) + wib;
-    if (pr >= n) return;
-    // per warp: prefix sums (L+1 doubles, squared cost only), zq, zs (L floats each)
-    const size_t wbytes = (EU ? 8 * (size_t)(L + 1) : 0) + 8 * (size_t)L;
-    double* P = (double*)(bsm + (size_t)wib * round_up((int64_t)wbytes, 16));
+    __shared__ double red[8];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int64_t pr = BLOCK ? (int64_t)blockIdx.x : (int64_t)blockIdx.x * (blockDim.x >> 5) + wid;
+    if (pr >= n) return;  // whole scope
+    const int me = BLOCK ? (int)threadIdx.x : lane;
+    const int step = BLOCK ? (int)blockDim.x : 32;
+    auto sync = [] {
+        if (BLOCK) __syncthreads();
+        else __syncwarp();
+    };
+    const size_t wbytes = (size_t)round_up((int64_t)((EU ? 8 * (size_t)(L + 1) : 0) + 8 * (size_t)L), 16);
+    double* P = (double*)(bsm + (BLOCK ? 0 : (size_t)wid * wbytes));  // L + 1 (squared cost)
     float* zqs = (float*)(P + (EU ? L + 1 : 0));
     float* zss = zqs + L;
     const bool zn = hdr != nullptr;
@@ -464,12 +525,12 @@ pair_bwd_kernel(const float* __restrict__ q, const float* __restrict__ s, int64_
     }
     const float* xq = q + pr * L;
     const float* xs = s + pr * L;
-    for (int t = lane; t < L; t += 32) {
+    for (int t = me; t < L; t += step) {
         const float a = __ldg(xq + t), b = __ldg(xs + t);
         zqs[t] = zn ? pair_z(a, muq, invq) : a;
         zss[t] = zn ? pair_z(b, mus, invs) : b;
     }
-    __syncwarp();
+    sync();
     auto fp = [](float df) { return df > 0.f ? 1.0f : (df < 0.f ? -1.0f : 0.0f); };
     const float up = dD ? __ldg(dD + pr) : 1.0f;
     for (int side = 0; side < 2; ++side) {
@@ -479,48 +540,50 @@ pair_bwd_kernel(const float* __restrict__ q, const float* __restrict__ s, int64_
         const uint32_t* run = (side == 0 ? rows : cols) + pr * L;
         const float* zt_s = side == 0 ? zqs : zss;
         const float* zo_s = side == 0 ? zss : zqs;
-        if (EU) warp_prefix(zo_s, P, L, lane);
+        if (EU) {
+            if (BLOCK) block_prefix(zo_s, P, L, red);
+            else warp_prefix(zo_s, P, L, lane);
+        }
         double sg = 0.0, sgz = 0.0;
-        for (int t0 = lane; t0 < L; t0 += 4 * 32) {
-            uint32_t r[4];  // four runs in flight per lane
-#pragma unroll
-            for (int v = 0; v < 4; ++v) r[v] = t0 + 32 * v < L ? __ldg(run + t0 + 32 * v) : 0u;
-#pragma unroll
-            for (int v = 0; v < 4; ++v) {
-                const int t = t0 + 32 * v;
-                if (t >= L) break;
-                const int hi = min((int)(r[v] >> 16), L - 1);
-                const int lo = min((int)(r[v] & 0xffffu), hi);
-                const float zt = zt_s[t];
-                float g;
-                if (EU) {
-                    // q side: sum_j 2 (zq_t - zs_j); s side: -sum_i 2 (zq_i - zs_t)
-                    // = sum_i 2 (zs_t - zq_i): both 2 (len z_t - sum of the other)
-                    const double sum = (double)(hi - lo + 1) * (double)zt - (P[hi + 1] - P[lo]);
-                    g = (float)(2.0 * sum);
-                } else {
-                    g = 0.f;
-                    for (int u = lo; u <= hi; ++u) {
-                        const float o = zo_s[u];
-                        g += side == 0 ? fp(__fsub_rn(zt, o)) : -fp(__fsub_rn(o, zt));
-                    }
+        for (int t = me; t < L; t += step) {
+            const uint32_t r = __ldg(run + t);
+            const int hi = min((int)(r >> 16), L - 1);
+            const int lo = min((int)(r & 0xffffu), hi);
+            const float zt = zt_s[t];
+            float g;
+            if (EU) {
+                // q side: sum_j 2 (zq_t - zs_j); s side: -sum_i 2 (zq_i - zs_t)
+                // = sum_i 2 (zs_t - zq_i): both 2 (len z_t - sum of the other)
+                const double sum = (double)(hi - lo + 1) * (double)zt - (P[hi + 1] - P[lo]);
+                g = (float)(2.0 * sum);
+            } else {
+                g = 0.f;
+                for (int u = lo; u <= hi; ++u) {
+                    const float o = zo_s[u];
+                    g += side == 0 ? fp(__fsub_rn(zt, o)) : -fp(__fsub_rn(o, zt));
                 }
-                out[t] = zn ? g : g * up;
-                sg += (double)g;
-                sgz += (double)g * (double)zt;
             }
+            out[t] = zn ? g : g * up;
+            sg += (double)g;
+            sgz += (double)g * (double)zt;
         }
-        __syncwarp();  // P is rebuilt for the other side
-        if (!zn) continue;
-        for (int o = 16; o > 0; o >>= 1) {
-            sg += __shfl_xor_sync(kFull, sg, o);
-            sgz += __shfl_xor_sync(kFull, sgz, o);
+        if (zn) {
+            if (BLOCK) {
+                block_sum2(sg, sgz, red);
+            } else {
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) {
+                    sg += __shfl_xor_sync(kFull, sg, o);
+                    sgz += __shfl_xor_sync(kFull, sgz, o);
+                }
+            }
+            const bool deg = side == 0 ? degq : degs;
+            const double inv = side == 0 ? invq : invs;
+            const double mg = sg / (double)L, mgz = deg ? 0.0 : sgz / (double)L;
+            for (int t = me; t < L; t += step)  // each thread re-reads its own values
+                out[t] = (float)((double)up * ((double)out[t] - mg - (double)zt_s[t] * mgz) * inv);
         }
-        const bool deg = side == 0 ? degq : degs;
-        const double inv = side == 0 ? invq : invs;
-        const double mg = sg / (double)L, mgz = deg ? 0.0 : sgz / (double)L;
-        for (int t = lane; t < L; t += 32)  // each lane re-reads its own values
-            out[t] = (float)((double)up * ((double)out[t] - mg - (double)zt_s[t] * mgz) * inv);
+        sync();  // P is rebuilt for the other side
     }
 }
 
@@ -620,17 +683,22 @@ int launch_pair_fwd(cdtw_handle h, const float* zq, const float* zs, int64_t n, 
 int launch_pair_bwd(cdtw_handle h, const float* q, const float* s, int64_t n, int L,
                     const double* hdr, const uint32_t* rows, const uint32_t* cols,
                     const float* dD, bool euclid, float* dq, float* ds) {
-    // per warp: z of both series (8L bytes) and, for the squared cost, one
-    // prefix-sum array (8(L+1) bytes); up to 4 warps in 96 KB
+    // per pair: z of both series (8L bytes) and, for the squared cost, one
+    // prefix-sum array (8(L+1) bytes); a warp per pair (up to 4 per block,
+    // 96 KB) for L <= 1024, a 4-warp block per pair above
     const size_t wbytes =
         (size_t)round_up((int64_t)((euclid ? 8 * (size_t)(L + 1) : 0) + 8 * (size_t)L), 16);
-    const int nw = (int)std::max<size_t>(1, std::min<size_t>(4, 96 * 1024 / wbytes));
-    const size_t smem = (size_t)nw * wbytes;
-    const int blocks = (int)div_up(n, nw);
-    auto k = euclid ? pair_bwd_kernel<true> : pair_bwd_kernel<false>;
+    const bool block = L > 1024;
+    const int nw = block ? 1 : (int)std::max<size_t>(1, std::min<size_t>(4, 96 * 1024 / wbytes));
+    const size_t smem = block ? wbytes : (size_t)nw * wbytes;
+    const int64_t blocks = block ? n : div_up(n, nw);
+    if (blocks > INT32_MAX) return set_error(h, CDTW_EINVAL, "too many pairs");
+    auto k = euclid ? (block ? pair_bwd_kernel<true, true> : pair_bwd_kernel<true, false>)
+                    : (block ? pair_bwd_kernel<false, true> : pair_bwd_kernel<false, false>);
     CDTW_CUDA(h, cudaFuncSetAttribute((const void*)k, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)smem));
-    k<<<blocks, nw * 32, smem, h->stream>>>(q, s, n, L, hdr, rows, cols, dD, dq, ds);
+    k<<<(unsigned)blocks, block ? kBwdThreads : nw * 32, smem, h->stream>>>(q, s, n, L, hdr, rows,
+                                                                           cols, dD, dq, ds);
     CDTW_LAUNCH(h, "pair_bwd_kernel");
     return CDTW_OK;
 }
