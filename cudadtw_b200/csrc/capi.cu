@@ -158,6 +158,10 @@ int cdtw_destroy(cdtw_handle h) {
     if (h->ring) cudaFree(h->ring);
     if (h->pinned) cudaFreeHost(h->pinned);
     if (h->own_stream) cudaStreamDestroy(h->own_stream);
+    if (h->xready) {
+        for (cudaStream_t st : h->xfer) cudaStreamDestroy(st);
+        for (cudaEvent_t ev : h->xev) cudaEventDestroy(ev);
+    }
     delete h;
     return CDTW_OK;
 }
@@ -256,14 +260,47 @@ int cdtw_all_windows_host(cdtw_handle h, const float* h_query, int M, const floa
     double* dmu = (double*)(base + o_mu);
     float* dsd = (float*)(base + o_sd);
     float* dout = (float*)(base + o_out);
-    CDTW_CUDA(h, cudaMemcpyAsync(dx, h_subject, sizeof(float) * N, cudaMemcpyHostToDevice,
-                                 h->stream));
     CDTW_TRY(cdtw_set_query(h, h_query, M, W, CDTW_HOST));
-    CDTW_TRY(launch_avg_std(h, dx, N, M, dmu, dsd));
-    CDTW_TRY(launch_cdtw_windows(h, dx, N, dmu, dsd, nullptr, Nw, metric == CDTW_EUCLIDEAN,
-                                 dout));
-    CDTW_CUDA(h, cudaMemcpyAsync(h_out, dout, sizeof(float) * Nw, cudaMemcpyDeviceToHost,
-                                 h->stream));
+    // pipeline over window chunks (multiples of the statistics kernel's
+    // 2048-window warp runs, so per-chunk statistics equal the whole-stream
+    // ones): samples in on xfer[0], statistics + cDTW on the handle's stream,
+    // results out on xfer[1]; chunk i's copies overlap chunk i-1's compute
+    if (!h->xready) {
+        for (cudaStream_t& st : h->xfer)
+            CDTW_CUDA(h, cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+        for (cudaEvent_t& ev : h->xev)
+            CDTW_CUDA(h, cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+        h->xready = true;
+    }
+    const int64_t run = 2048;
+    const int64_t chunk =
+        round_up(std::max<int64_t>(div_up(Nw, 16), std::min<int64_t>(Nw, (int64_t)1 << 19)), run);
+    const int nch = (int)div_up(Nw, chunk);
+    cudaEvent_t start = h->xev[3 * 16];
+    CDTW_CUDA(h, cudaEventRecord(start, h->stream));  // after earlier work on the workspace
+    CDTW_CUDA(h, cudaStreamWaitEvent(h->xfer[0], start, 0));
+    CDTW_CUDA(h, cudaStreamWaitEvent(h->xfer[1], start, 0));
+    const bool eu = metric == CDTW_EUCLIDEAN;
+    int64_t copied = 0;  // samples already on the device
+    for (int i = 0; i < nch; ++i) {
+        const int64_t c0 = (int64_t)i * chunk, c1 = std::min(Nw, c0 + chunk);
+        const int64_t s1 = c1 + M - 1;  // samples chunk i needs: [c0, s1)
+        cudaEvent_t in = h->xev[3 * i], done = h->xev[3 * i + 1];
+        CDTW_CUDA(h, cudaMemcpyAsync(dx + copied, h_subject + copied,
+                                     sizeof(float) * (s1 - copied), cudaMemcpyHostToDevice,
+                                     h->xfer[0]));
+        copied = s1;
+        CDTW_CUDA(h, cudaEventRecord(in, h->xfer[0]));
+        CDTW_CUDA(h, cudaStreamWaitEvent(h->stream, in, 0));
+        CDTW_TRY(launch_avg_std(h, dx + c0, s1 - c0, M, dmu + c0, dsd + c0));
+        CDTW_TRY(launch_cdtw_windows(h, dx + c0, s1 - c0, dmu + c0, dsd + c0, nullptr, c1 - c0,
+                                     eu, dout + c0));
+        CDTW_CUDA(h, cudaEventRecord(done, h->stream));
+        CDTW_CUDA(h, cudaStreamWaitEvent(h->xfer[1], done, 0));
+        CDTW_CUDA(h, cudaMemcpyAsync(h_out + c0, dout + c0, sizeof(float) * (c1 - c0),
+                                     cudaMemcpyDeviceToHost, h->xfer[1]));
+    }
+    CDTW_CUDA(h, cudaStreamSynchronize(h->xfer[1]));
     CDTW_CUDA(h, cudaStreamSynchronize(h->stream));
     return CDTW_OK;
 }

@@ -77,6 +77,11 @@ struct cdtw_handle_s {
     int64_t last_counts[4] = {0, 0, 0, 0};
     // cDTW kernel variant per band (0 = built-in rule); set by the autotuner
     unsigned char band_variant[CDTW_MAX_QUERY] = {0};
+    // host-buffer pipeline (cdtw_all_windows_host): copy-in / copy-out streams
+    // and an event pool, created on first use
+    cudaStream_t xfer[2] = {nullptr, nullptr};
+    cudaEvent_t xev[3 * 16 + 1] = {};
+    bool xready = false;
     char err[512] = {0};
 };
 

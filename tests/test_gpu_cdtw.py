@@ -154,3 +154,19 @@ def test_strip_kernel_index_list(handle):
     assert np.isnan(got[7])
     keep = np.arange(idx.size) != 7
     np.testing.assert_array_equal(got[keep], full[idx[keep]])
+
+
+@pytest.mark.parametrize("W", [12, 60, 120])
+def test_host_call_pipelined_chunks_equal_device_path(handle, W):
+    """cdtw_all_windows_host pipelines copies and compute over window chunks;
+    with chunk starts on the statistics kernel's 2048-window runs its results
+    are bit-identical to the device-buffer path (several chunks, ragged tail,
+    the two-window, one-window and strip kernels)."""
+    x = synth.metal_like((1 << 21) + 777, seed=9)
+    q, _ = synth.cut_query(x, 160, seed=10, noise=0.1)
+    dx = _dev(x)
+    avg, std = handle.avg_std(dx, q.size)
+    handle.set_query(q, W)
+    full = handle.gpu_cdtw(dx, avg, std).cpu().numpy()
+    host = handle.all_windows_host(q, x, W)
+    np.testing.assert_array_equal(host, full)
