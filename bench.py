@@ -376,6 +376,22 @@ def subresults(h, dev) -> dict:
                              "plain_s": tp, "speedup": tp / tb, "same_location": same,
                              "note": "plain excludes the per-length statistics (shared)"}
     del dx
+    # many short queries on a short stream: the regime where the per-search
+    # launches and host round trips of the plain path dominate
+    x = synth.ecg_like(1 << 20, seed=1)
+    dx = torch.from_numpy(x).to(dev)
+    batch = synth.batch_queries(x, 512, seed=3, m_lo=64, m_hi=128)
+    qs = [b[0] for b in batch]
+    ws = [b[1] for b in batch]
+    h.search_batched(dx, qs, ws)
+    tb, (bl, bd) = dev_time(lambda: h.search_batched(dx, qs, ws))
+    stats = {m: h.avg_std(dx, m) for m in sorted({q.size for q in qs})}
+    tp, pres = dev_time(plain)
+    same = sum(int(a == r[0]) for a, r in zip(bl, pres))
+    out["batched_search_short"] = {"queries": len(qs), "stream": "ecg 2^20", "M": [64, 128],
+                                   "batched_s": tb, "plain_s": tp, "speedup": tp / tb,
+                                   "same_location": same}
+    del dx
 
     # -- pair forward / backward ------------------------------------------
     pair = {}
@@ -476,7 +492,8 @@ def refine_subresult(h, dev) -> dict:
 
 def profile_case(name: str) -> None:
     """One small run of a scope row (twice, untimed) for an ncu capture:
-    search = config-1 pruned search (2^25 metal-like, M=512, P=10); topk =
+    search = config-1 pruned search (2^25 metal-like, M=512, P=10); strip =
+    all-windows cDTW of 2^18 windows at M=1024, W=204 (strip kernel); topk =
     top-1000 of one M=256 template on a 2^22 ECG-like stream; pair = 256 pairs
     of L=2048, W=409 and 4096 pairs of L=256, W=25 (forward, forward with path,
     backward); refine = 8 templates x 200 matches, 5 Adam steps."""
@@ -499,6 +516,13 @@ def profile_case(name: str) -> None:
                 avg, std = h.avg_std(dx, 256)
                 h.set_query(q, 25)
                 h.topk(dx, avg, std, 1000)
+            elif name == "strip":
+                x = synth.metal_like((1 << 18) + 1023, seed=1)
+                dx = torch.from_numpy(x).to(dev)
+                q, _ = synth.cut_query(x, 1024, seed=5, noise=0.1)
+                avg, std = h.avg_std(dx, 1024)
+                h.set_query(q, 204)
+                h.gpu_cdtw(dx, avg, std)
             elif name == "pair":
                 for n, L, W in ((256, 2048, 409), (4096, 256, 25)):
                     rng = np.random.default_rng(0)
@@ -544,7 +568,7 @@ def main() -> None:
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--profile", choices=["search", "topk", "pair", "refine"],
+    ap.add_argument("--profile", choices=["search", "topk", "pair", "refine", "strip"],
                     help="run one small case of that row twice (for ncu) and exit")
     ap.add_argument("--no-sub", action="store_true",
                     help="skip the pruned / batched search and pair fwd/bwd sub-results")
