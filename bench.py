@@ -493,7 +493,9 @@ def refine_subresult(h, dev) -> dict:
 def profile_case(name: str) -> None:
     """One small run of a scope row (twice, untimed) for an ncu capture:
     search = config-1 pruned search (2^25 metal-like, M=512, P=10); strip =
-    all-windows cDTW of 2^18 windows at M=1024, W=204 (strip kernel); topk =
+    all-windows cDTW of 2^18 windows at M=1024, W=204 (strip kernel);
+    batch_short = the batched search of 512 queries (M 64-128) on a 2^20 ECG-like
+    stream; topk =
     top-1000 of one M=256 template on a 2^22 ECG-like stream; pair = 256 pairs
     of L=2048, W=409 and 4096 pairs of L=256, W=25 (forward, forward with path,
     backward); refine = 8 templates x 200 matches, 5 Adam steps."""
@@ -516,6 +518,11 @@ def profile_case(name: str) -> None:
                 avg, std = h.avg_std(dx, 256)
                 h.set_query(q, 25)
                 h.topk(dx, avg, std, 1000)
+            elif name == "batch_short":
+                x = synth.ecg_like(1 << 20, seed=1)
+                dx = torch.from_numpy(x).to(dev)
+                batch = synth.batch_queries(x, 512, seed=3, m_lo=64, m_hi=128)
+                h.search_batched(dx, [b[0] for b in batch], [b[1] for b in batch])
             elif name == "strip":
                 x = synth.metal_like((1 << 18) + 1023, seed=1)
                 dx = torch.from_numpy(x).to(dev)
@@ -568,7 +575,8 @@ def main() -> None:
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--profile", choices=["search", "topk", "pair", "refine", "strip"],
+    ap.add_argument("--profile",
+                    choices=["search", "topk", "pair", "refine", "strip", "batch_short"],
                     help="run one small case of that row twice (for ncu) and exit")
     ap.add_argument("--no-sub", action="store_true",
                     help="skip the pruned / batched search and pair fwd/bwd sub-results")
