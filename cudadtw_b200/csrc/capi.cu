@@ -263,8 +263,9 @@ int cdtw_all_windows_host(cdtw_handle h, const float* h_query, int M, const floa
     CDTW_TRY(cdtw_set_query(h, h_query, M, W, CDTW_HOST));
     // pipeline over window chunks (multiples of the statistics kernel's
     // 2048-window warp runs, so per-chunk statistics equal the whole-stream
-    // ones): samples in on xfer[0], statistics + cDTW on the handle's stream,
-    // results out on xfer[1]; chunk i's copies overlap chunk i-1's compute
+    // ones): samples in on xfer[0], statistics + cDTW alternately on the
+    // handle's stream and xfer[2] (a chunk's first waves overlap the previous
+    // chunk's last), results out on xfer[1]; copies overlap compute
     if (!h->xready) {
         for (cudaStream_t& st : h->xfer)
             CDTW_CUDA(h, cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
@@ -278,9 +279,12 @@ int cdtw_all_windows_host(cdtw_handle h, const float* h_query, int M, const floa
     const int nch = (int)div_up(Nw, chunk);
     cudaEvent_t start = h->xev[3 * 16];
     CDTW_CUDA(h, cudaEventRecord(start, h->stream));  // after earlier work on the workspace
-    CDTW_CUDA(h, cudaStreamWaitEvent(h->xfer[0], start, 0));
-    CDTW_CUDA(h, cudaStreamWaitEvent(h->xfer[1], start, 0));
+    for (cudaStream_t st : h->xfer) CDTW_CUDA(h, cudaStreamWaitEvent(st, start, 0));
     const bool eu = metric == CDTW_EUCLIDEAN;
+    cudaStream_t const user = h->stream;
+    // strip kernels share the handle's ring buffer: their chunks stay on one stream
+    const bool alternate = choose_variant(h, h->q.W) == CDTW_VARIANT_REGISTER;
+    cudaStream_t const comp[2] = {user, alternate ? h->xfer[2] : user};
     int64_t copied = 0;  // samples already on the device
     for (int i = 0; i < nch; ++i) {
         const int64_t c0 = (int64_t)i * chunk, c1 = std::min(Nw, c0 + chunk);
@@ -291,16 +295,21 @@ int cdtw_all_windows_host(cdtw_handle h, const float* h_query, int M, const floa
                                      h->xfer[0]));
         copied = s1;
         CDTW_CUDA(h, cudaEventRecord(in, h->xfer[0]));
-        CDTW_CUDA(h, cudaStreamWaitEvent(h->stream, in, 0));
-        CDTW_TRY(launch_avg_std(h, dx + c0, s1 - c0, M, dmu + c0, dsd + c0));
-        CDTW_TRY(launch_cdtw_windows(h, dx + c0, s1 - c0, dmu + c0, dsd + c0, nullptr, c1 - c0,
-                                     eu, dout + c0));
-        CDTW_CUDA(h, cudaEventRecord(done, h->stream));
+        h->stream = comp[i & 1];
+        int st = cudaStreamWaitEvent(h->stream, in, 0) == cudaSuccess ? CDTW_OK : CDTW_ECUDA;
+        if (st == CDTW_OK) st = launch_avg_std(h, dx + c0, s1 - c0, M, dmu + c0, dsd + c0);
+        if (st == CDTW_OK)
+            st = launch_cdtw_windows(h, dx + c0, s1 - c0, dmu + c0, dsd + c0, nullptr, c1 - c0,
+                                     eu, dout + c0);
+        if (st == CDTW_OK && cudaEventRecord(done, h->stream) != cudaSuccess) st = CDTW_ECUDA;
+        h->stream = user;
+        if (st != CDTW_OK) return st == CDTW_ECUDA ? check_cuda(h, cudaGetLastError(), "pipeline") : st;
         CDTW_CUDA(h, cudaStreamWaitEvent(h->xfer[1], done, 0));
         CDTW_CUDA(h, cudaMemcpyAsync(h_out + c0, dout + c0, sizeof(float) * (c1 - c0),
                                      cudaMemcpyDeviceToHost, h->xfer[1]));
     }
     CDTW_CUDA(h, cudaStreamSynchronize(h->xfer[1]));
+    CDTW_CUDA(h, cudaStreamSynchronize(h->xfer[2]));
     CDTW_CUDA(h, cudaStreamSynchronize(h->stream));
     return CDTW_OK;
 }

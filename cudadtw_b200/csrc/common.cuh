@@ -77,9 +77,9 @@ struct cdtw_handle_s {
     int64_t last_counts[4] = {0, 0, 0, 0};
     // cDTW kernel variant per band (0 = built-in rule); set by the autotuner
     unsigned char band_variant[CDTW_MAX_QUERY] = {0};
-    // host-buffer pipeline (cdtw_all_windows_host): copy-in / copy-out streams
-    // and an event pool, created on first use
-    cudaStream_t xfer[2] = {nullptr, nullptr};
+    // host-buffer pipeline (cdtw_all_windows_host): copy-in, copy-out and a
+    // second compute stream, and an event pool, created on first use
+    cudaStream_t xfer[3] = {nullptr, nullptr, nullptr};
     cudaEvent_t xev[3 * 16 + 1] = {};
     bool xready = false;
     char err[512] = {0};
