@@ -74,8 +74,11 @@ lb_kim_kernel(const float* __restrict__ x, const double* __restrict__ mu,
 // place up to the largest power of two p <= K = 2W+1, and output t takes the
 // spans starting at t and at t + K - p.  Coalesced in and out, no scratch.
 constexpr int kEnvThreads = 512;
-constexpr int kEnvSmemFloats = 50176;  // both arrays: 196 KB
+constexpr int kEnvSmemFloats = 50176;  // 196 KB
 
+// PING: two buffers per extremum, one barrier per doubling pass (when they
+// fit); otherwise one buffer updated in place in increasing chunks.
+template <bool PING>
 __global__ void __launch_bounds__(kEnvThreads)
 env_window_kernel(const float* __restrict__ x, int64_t N, int W, int T, float2* __restrict__ env) {
     extern __shared__ float esm[];
@@ -83,6 +86,8 @@ env_window_kernel(const float* __restrict__ x, int64_t N, int W, int T, float2* 
     const int S = T + 2 * W;
     float* lo = esm;
     float* hi = esm + S;
+    float* lo2 = esm + 2 * S;  // PING only
+    float* hi2 = esm + 3 * S;
     const int64_t t0 = (int64_t)blockIdx.x * T;
     for (int i = threadIdx.x; i < S; i += kEnvThreads) {
         const int64_t g = t0 - W + i;
@@ -94,21 +99,37 @@ env_window_kernel(const float* __restrict__ x, int64_t N, int W, int T, float2* 
     __syncthreads();
     int p = 1;
     for (; 2 * p <= K; p *= 2) {
-        // entry i becomes the extremum of [i, i + 2p); chunks in increasing i,
-        // so a partner i + p > i is never one this pass already rewrote
-        for (int i0 = 0; i0 < S - p; i0 += kEnvThreads) {
-            const int i = i0 + threadIdx.x;
-            float a = 0.f, b = 0.f;
-            if (i < S - p) {
-                a = fminf(lo[i], lo[i + p]);
-                b = fmaxf(hi[i], hi[i + p]);
+        // entry i becomes the extremum of [i, i + 2p)
+        if (PING) {
+            for (int i = threadIdx.x; i < S; i += kEnvThreads) {
+                const int j = min(i + p, S - 1);
+                lo2[i] = fminf(lo[i], lo[j]);
+                hi2[i] = fmaxf(hi[i], hi[j]);
             }
             __syncthreads();
-            if (i < S - p) {
-                lo[i] = a;
-                hi[i] = b;
+            float* t = lo;
+            lo = lo2;
+            lo2 = t;
+            t = hi;
+            hi = hi2;
+            hi2 = t;
+        } else {
+            // chunks in increasing i, so a partner i + p > i is never one this
+            // pass already rewrote
+            for (int i0 = 0; i0 < S - p; i0 += kEnvThreads) {
+                const int i = i0 + threadIdx.x;
+                float a = 0.f, b = 0.f;
+                if (i < S - p) {
+                    a = fminf(lo[i], lo[i + p]);
+                    b = fmaxf(hi[i], hi[i + p]);
+                }
+                __syncthreads();
+                if (i < S - p) {
+                    lo[i] = a;
+                    hi[i] = b;
+                }
+                __syncthreads();
             }
-            __syncthreads();
         }
     }
     for (int t = threadIdx.x; t < T; t += kEnvThreads) {
@@ -179,15 +200,22 @@ size_t stream_envelope_scratch_bytes(int64_t) { return 0; }
 
 int launch_stream_envelope(cdtw_handle h, const float* x, int64_t N, int W, float*,
                            float2* env) {
-    // tile: at least 2048 outputs (or 2W when the halo is larger), within the
-    // shared-memory budget of both arrays
-    const int T = std::max(1, std::min(std::max(2048, 2 * W), kEnvSmemFloats / 2 - 2 * W));
+    // tile: at least 2048 outputs (or 2W when the halo is larger); four
+    // arrays (ping-pong) when they fit the shared-memory budget, else two
     if (kEnvSmemFloats / 2 - 2 * W < 1)
         return set_error(h, CDTW_EUNSUPPORTED, "band W=%d too wide for the stream envelope", W);
-    const size_t smem = (size_t)2 * (T + 2 * W) * sizeof(float);
-    CDTW_CUDA(h, cudaFuncSetAttribute((const void*)env_window_kernel,
-                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    env_window_kernel<<<(unsigned)div_up(N, T), kEnvThreads, smem, h->stream>>>(x, N, W, T, env);
+    const bool ping = kEnvSmemFloats / 4 - 2 * W >= 2048;
+    const int arrays = ping ? 4 : 2;
+    const int T = std::max(1, std::min(std::max(2048, 2 * W), kEnvSmemFloats / arrays - 2 * W));
+    const size_t smem = (size_t)arrays * (T + 2 * W) * sizeof(float);
+    const void* k = ping ? (const void*)env_window_kernel<true> : (const void*)env_window_kernel<false>;
+    CDTW_CUDA(h, cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    if (ping)
+        env_window_kernel<true><<<(unsigned)div_up(N, T), kEnvThreads, smem, h->stream>>>(x, N, W, T,
+                                                                                     env);
+    else
+        env_window_kernel<false><<<(unsigned)div_up(N, T), kEnvThreads, smem, h->stream>>>(x, N, W,
+                                                                                      T, env);
     CDTW_LAUNCH(h, "env_window_kernel");
     return CDTW_OK;
 }

@@ -4,10 +4,11 @@
 // the whole stream (CUB scans, 2 cudaMalloc + 5 kernels per 1e7-sample epoch,
 // stats.cuh:85-142) and then takes the variance in FP32 (stats.cuh:49), which
 // loses the variance of level-shifted signals.  Here one kernel reads the
-// stream once: each warp owns a run of consecutive windows, keeps FP64 sums
-// of (x-c) and (x-c)^2 for a warp-local shift c, and slides them 32 windows
-// per round with a warp scan of the entering-minus-leaving terms.  Output per
-// window: mean (FP64) and sigma (FP32), 12 bytes.
+// stream once: each warp owns a run of consecutive windows in four
+// sub-runs, keeps FP64 sums of (x-c) and (x-c)^2 for a shift c per sub-run,
+// and slides them 32 windows per round with warp scans of the
+// entering-minus-leaving terms (the four sub-runs' scans interleaved).
+// Output per window: mean (FP64) and sigma (FP32), 12 bytes.
 #include "common.cuh"
 
 namespace cdtw {
@@ -17,7 +18,7 @@ namespace {
 constexpr int kStatsRounds = 64;                 // rounds of 32 windows per warp
 constexpr int kStatsWarpWindows = 32 * kStatsRounds;
 constexpr int kStatsBlock = 128;                 // 4 warps per block
-constexpr int kStatsBatch = 8;                   // rounds whose samples load together
+constexpr int kStatsSub = 4;                     // interleaved sub-runs per warp
 
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll
@@ -25,69 +26,91 @@ __device__ __forceinline__ double warp_sum(double v) {
     return v;
 }
 
-__device__ __forceinline__ double warp_incl_scan(double v, int lane) {
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const double t = __shfl_up_sync(0xffffffffu, v, o);
-        if (lane >= o) v += t;
-    }
-    return v;
-}
-
 template <class XT, class ST>
 __global__ void __launch_bounds__(kStatsBlock)
 avg_std_kernel(const XT* __restrict__ x, int64_t N, int M, double* __restrict__ mu,
                ST* __restrict__ sigma) {
+    // The warp's run of kStatsWarpWindows windows is split into kStatsSub
+    // sub-runs, each with its own shift c and starting sums; their scans are
+    // interleaved round by round (independent shuffle / FP64 chains).
     const int64_t Nw = N - M + 1;
     const int lane = threadIdx.x & 31;
     const int64_t warp = (int64_t)blockIdx.x * (kStatsBlock / 32) + (threadIdx.x >> 5);
     const int64_t a = warp * kStatsWarpWindows;
     if (a >= Nw) return;
-    const double c = (double)x[a];
-    // sums of the first window of the run
-    double s1 = 0.0, s2 = 0.0;
-    for (int k = lane; k < M; k += 32) {
-        const double v = (double)x[a + k] - c;
-        s1 += v;
-        s2 = fma(v, v, s2);
+    constexpr int kSubRounds = kStatsRounds / kStatsSub;
+    constexpr int kSubWindows = 32 * kSubRounds;
+    double c[kStatsSub], s1[kStatsSub], s2[kStatsSub];
+#pragma unroll
+    for (int u = 0; u < kStatsSub; ++u) {
+        const int64_t as = min(a + (int64_t)u * kSubWindows, Nw - 1);
+        c[u] = (double)x[as];
+        s1[u] = 0.0;
+        s2[u] = 0.0;
     }
-    s1 = warp_sum(s1);
-    s2 = warp_sum(s2);
-    const double invM = 1.0 / (double)M;
-    // the entering / leaving samples of kStatsBatch rounds are loaded together
-    // (one memory latency per batch instead of one per round)
-    for (int r0 = 0; r0 < kStatsRounds; r0 += kStatsBatch) {
-        if (a + (int64_t)r0 * 32 >= Nw) break;  // warp-uniform
-        XT xin[kStatsBatch], xout[kStatsBatch];
+    // sums of the first window of every sub-run
+    for (int k = lane; k < M; k += 32) {
 #pragma unroll
-        for (int u = 0; u < kStatsBatch; ++u) {
-            const int64_t w = a + (int64_t)(r0 + u) * 32 + lane;
-            const bool ok = w < Nw - 1;
-            xin[u] = ok ? x[w + M] : (XT)0;
-            xout[u] = ok ? x[w] : (XT)0;
+        for (int u = 0; u < kStatsSub; ++u) {
+            const int64_t as = min(a + (int64_t)u * kSubWindows, Nw - 1);
+            const double v = (double)x[as + k] - c[u];
+            s1[u] += v;
+            s2[u] = fma(v, v, s2[u]);
         }
+    }
 #pragma unroll
-        for (int u = 0; u < kStatsBatch; ++u) {
-            const int64_t w = a + (int64_t)(r0 + u) * 32 + lane;
-            if (a + (int64_t)(r0 + u) * 32 >= Nw) break;  // warp-uniform
-            double d1 = 0.0, d2 = 0.0;
+    for (int u = 0; u < kStatsSub; ++u) {
+        s1[u] = warp_sum(s1[u]);
+        s2[u] = warp_sum(s2[u]);
+    }
+    const double invM = 1.0 / (double)M;
+    for (int r = 0; r < kSubRounds; ++r) {
+        if (a + (int64_t)r * 32 >= Nw) break;  // warp-uniform (sub-run 0 ends first)
+        double d1[kStatsSub], d2[kStatsSub];
+        int64_t wv[kStatsSub];
+#pragma unroll
+        for (int u = 0; u < kStatsSub; ++u) {
+            const int64_t w = a + (int64_t)u * kSubWindows + (int64_t)r * 32 + lane;
+            wv[u] = w;
+            d1[u] = 0.0;
+            d2[u] = 0.0;
             if (w < Nw - 1) {
                 // window w+1 = window w + x[w+M] - x[w]
-                const double vin = (double)xin[u] - c, vout = (double)xout[u] - c;
-                d1 = vin - vout;
-                d2 = vin * vin - vout * vout;
+                const double vin = (double)x[w + M] - c[u], vout = (double)x[w] - c[u];
+                d1[u] = vin - vout;
+                d2[u] = vin * vin - vout * vout;
             }
-            const double i1 = warp_incl_scan(d1, lane), i2 = warp_incl_scan(d2, lane);
+        }
+        double i1[kStatsSub], i2[kStatsSub];
+#pragma unroll
+        for (int u = 0; u < kStatsSub; ++u) {
+            i1[u] = d1[u];
+            i2[u] = d2[u];
+        }
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+#pragma unroll
+            for (int u = 0; u < kStatsSub; ++u) {
+                const double t1 = __shfl_up_sync(0xffffffffu, i1[u], o);
+                const double t2 = __shfl_up_sync(0xffffffffu, i2[u], o);
+                if (lane >= o) {
+                    i1[u] += t1;
+                    i2[u] += t2;
+                }
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < kStatsSub; ++u) {
             // sums of window w: base + exclusive scan
-            const double w1 = s1 + (i1 - d1), w2 = s2 + (i2 - d2);
-            if (w < Nw) {
+            const double w1 = s1[u] + (i1[u] - d1[u]), w2 = s2[u] + (i2[u] - d2[u]);
+            if (wv[u] < Nw) {
                 const double m1 = w1 * invM;
                 const double var = w2 * invM - m1 * m1;
-                mu[w] = c + m1;
-                sigma[w] = var > 0.0 ? (ST)sqrt(var) : (ST)1;
+                mu[wv[u]] = c[u] + m1;
+                sigma[wv[u]] = var > 0.0 ? (ST)sqrt(var) : (ST)1;
             }
-            s1 += __shfl_sync(0xffffffffu, i1, 31);
-            s2 += __shfl_sync(0xffffffffu, i2, 31);
+            s1[u] += __shfl_sync(0xffffffffu, i1[u], 31);
+            s2[u] += __shfl_sync(0xffffffffu, i2[u], 31);
         }
     }
 }
