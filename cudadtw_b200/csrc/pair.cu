@@ -14,13 +14,16 @@
 // the edge lanes reading the pair's series from global memory (L2-resident).
 //
 // With a path record the forward also stores 2 bits per band cell (diagonal
-// predecessor is the minimum; up <= left) in device scratch and, once the
-// pair is done, one lane backtracks from (L-1, L-1) to (0, 0) and writes the
-// warping path as row runs [a_i, b_i] and column runs [c_j, d_j].  Backward
+// predecessor is the minimum; up <= left) in device scratch, one element of
+// 2C bits per lane and anti-diagonal (a byte for C <= 4, 16 bits for C <= 8,
+// else 32), and, once the pair is done, one lane backtracks from (L-1, L-1)
+// to (0, 0) and writes the warping path as row runs [a_i, b_i] and column
+// runs [c_j, d_j].  Backward
 // sums the cost derivatives over those runs and applies the z-normalisation
 // Jacobian (I - 11'/L - zz'/L) / sigma.
 #include "common.cuh"
 
+#include <type_traits>
 #include <utility>
 
 namespace cdtw {
@@ -28,7 +31,7 @@ namespace cdtw {
 namespace {
 
 constexpr int kPairThreads = 128;
-constexpr int kWalkRows = 16;  // direction rows staged per backtracking chunk
+constexpr int kWalkChunk = 64;  // bytes of direction record per lane in one backtracking chunk
 constexpr unsigned kFull = 0xffffffffu;
 
 struct PairArgs {
@@ -37,8 +40,9 @@ struct PairArgs {
     int64_t n;
     int L, W, G, lgG;
     float* D;             // n outputs
-    uint32_t* dirs;       // per pair nkb x G words (path record only)
-    int nkb;
+    uint32_t* dirs;       // per pair dstride words: 2L-1 rows of G lane elements (path record)
+    int dstride;
+    int recb, logb;       // shared-record mode: bytes of record and move log per group
     uint32_t* rows;       // per pair L words: a_i | b_i << 16
     uint32_t* cols;       // per pair L words: c_j | d_j << 16
 };
@@ -58,6 +62,10 @@ __device__ __forceinline__ void dir_bits(uint32_t& w, float diag, float m, float
     asm("{\n\t.reg .pred p;\n\tsetp.le.f32 p, %1, %2;\n\t@p or.b32 %0, %0, %3;\n\t}"
         : "+r"(w) : "f"(up), "f"(left), "n"(2u << SH));
 }
+
+// Direction element of one lane and anti-diagonal: 2 bits per slot.
+template <int C>
+using DirT = std::conditional_t<(C <= 4), uint8_t, std::conditional_t<(C <= 8), uint16_t, uint32_t>>;
 
 // One cell (compile-time slot c) of an anti-diagonal of parity E.
 template <int C, bool EU, bool DIRS, int E, int RQ, int RS, int c>
@@ -93,32 +101,25 @@ __device__ __forceinline__ void dp_cells(float (&X)[C], const float (&Y)[C], con
     uint32_t nbits = 0;
     dp_cells_seq<C, EU, DIRS, E, RQ, RS>(X, Y, Q, Sv, lim, nb, nbits,
                                          std::make_integer_sequence<int, C>{});
-    if (DIRS) bits = (2 * C >= 32) ? nbits : ((bits << (2 * C)) | nbits);
+    if (DIRS) bits = nbits;
 }
 
 // State of one lane of a pair's group during the forward DP.
 template <int C>
 struct PairLane {
     float A[C], B[C], Q[C], Sv[C], lim[C];
-    uint32_t bits;
-    int u, kb;     // step within the current direction word, word row
+    uint32_t bits;  // direction bits of the last anti-diagonal
     int iq, js;    // lane 0's slot-0 query index, lane G-1's last-slot subject index
     float pq, ps;  // the values at iq + 1 / js + 1 (the next shift's)
 };
 
-template <int C, bool DIRS>
-__device__ __forceinline__ void flush_bits(PairLane<C>& st, uint32_t* drow, int G, int l, int k,
-                                           int K, bool live) {
-    constexpr int S = 16 / C;
-    if (!DIRS) return;
-    if (++st.u == S || k == K - 1) {
-        uint32_t w = st.bits;
-        const int pad = S - st.u;
-        if (pad > 0) w <<= 2 * C * pad;
-        if (live) drow[(size_t)st.kb * G + l] = w;
-        st.bits = 0;
-        st.u = 0;
-        ++st.kb;
+// Direction element of anti-diagonal k: to the pair's global record (DM 1,
+// live groups only) or to the group's shared-memory record (DM 2).
+template <int C, int DM>
+__device__ __forceinline__ void store_dirs(const PairLane<C>& st, uint32_t* drow, int G, int l,
+                                           int k, bool live) {
+    if constexpr (DM != 0) {
+        if (DM == 2 || live) ((DirT<C>*)drow)[(size_t)k * G + l] = (DirT<C>)st.bits;
     }
 }
 
@@ -160,26 +161,29 @@ __device__ __forceinline__ void step_even(PairLane<C>& st, const float* sq, int 
 }
 
 // 2C steps (C odd/even pairs) starting with an odd step at k; rotations
-// return to 0 at the end.  Stops at K.
-template <int C, bool EU, bool DIRS, int R>
+// return to 0 at the end.  CHK: stop at K (else the caller guarantees
+// k + 2C <= K).
+template <int C, bool EU, int DM, bool CHK, int R>
 __device__ __forceinline__ void body(PairLane<C>& st, const float* sq, const float* ss,
                                      uint32_t* drow, int L, int G, int l, int& k, int K,
                                      bool live) {
     if constexpr (R < C) {
-        if (k >= K) return;
+        constexpr bool DIRS = DM != 0;
+        if (CHK && k >= K) return;
         step_odd<C, EU, DIRS, R, R + 1>(st, ss, L, G, l, true);
-        flush_bits<C, DIRS>(st, drow, G, l, k, K, live);
-        if (++k >= K) return;
-        step_even<C, EU, DIRS, R + 1, R + 1>(st, sq, L, G, l, true);
-        flush_bits<C, DIRS>(st, drow, G, l, k, K, live);
+        store_dirs<C, DM>(st, drow, G, l, k, live);
         ++k;
-        body<C, EU, DIRS, R + 1>(st, sq, ss, drow, L, G, l, k, K, live);
+        if (CHK && k >= K) return;
+        step_even<C, EU, DIRS, R + 1, R + 1>(st, sq, L, G, l, true);
+        store_dirs<C, DM>(st, drow, G, l, k, live);
+        ++k;
+        body<C, EU, DM, CHK, R + 1>(st, sq, ss, drow, L, G, l, k, K, live);
     }
 }
 
-__device__ __forceinline__ void cp_async4(void* dst, const void* src) {
+__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
     const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(d), "l"(src) : "memory");
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(src) : "memory");
 }
 __device__ __forceinline__ void cp_async_commit() {
     asm volatile("cp.async.commit_group;" ::: "memory");
@@ -190,10 +194,185 @@ __device__ __forceinline__ void cp_async_wait() {
 }
 
 constexpr int kWalkStages = 4;            // direction chunks in flight during backtracking
-constexpr int kMoveLog = kWalkRows * 16;  // bytes: the moves of one chunk (<= kWalkRows * S)
+constexpr int kMoveLog = 256;             // bytes: the moves of one chunk (<= kWalkChunk)
+constexpr size_t kSharedRecMax = 76 * 1024;  // shared-record mode: bytes per block (3 per SM)
 
-template <int C, bool EU, bool DIRS>
+// Row runs (a_i, b_i) and column runs (c_j, d_j) of the moves mlog[m0 ..
+// m0 + nmax) of the group, lane l taking V consecutive moves; (gi, gj) is the
+// (group-uniform) cell before move m0 and is advanced past the moves.  Every
+// lane of the warp calls with the same nmax (full-mask shuffles).
+template <int V>
+__device__ __forceinline__ void runs_from_moves(const uint8_t* mlog, int nm, int nmax, int G,
+                                                int l, bool live, int L, uint16_t* r16,
+                                                uint16_t* c16, int& gi, int& gj) {
+    for (int m0 = 0; m0 < nmax; m0 += V * G) {
+        uint32_t bv[V];
+        int nr = 0, nc = 0;
+#pragma unroll
+        for (int v = 0; v < V; ++v) {
+            const int m = m0 + V * l + v;
+            bv[v] = m < nm ? mlog[m] : 4u;  // 4: no move
+            nr += (bv[v] != 0u && bv[v] != 4u) ? 1 : 0;  // leaves its row
+            nc += (bv[v] != 2u && bv[v] != 4u) ? 1 : 0;  // leaves its column
+        }
+        int sr = nr, sc = nc;  // inclusive scans over the group
+        for (int o = 1; o < G; o <<= 1) {
+            const int tr = __shfl_up_sync(kFull, sr, o, G);
+            const int tc = __shfl_up_sync(kFull, sc, o, G);
+            if (l >= o) {
+                sr += tr;
+                sc += tc;
+            }
+        }
+        int ib = gi - (sr - nr), jb = gj - (sc - nc);  // cell before this lane's first move
+#pragma unroll
+        for (int v = 0; v < V; ++v) {
+            const uint32_t b = bv[v];
+            const int lr = (b != 0u && b != 4u) ? 1 : 0;
+            const int lc = (b != 2u && b != 4u) ? 1 : 0;
+            const bool inside = live && (unsigned)ib < (unsigned)L && (unsigned)jb < (unsigned)L;
+            if (inside && lr) {
+                r16[2 * ib] = (uint16_t)jb;                               // a_i
+                if (ib > 0) r16[2 * (ib - 1) + 1] = (uint16_t)(jb - lc);  // b_(i-1)
+            }
+            if (inside && lc) {
+                c16[2 * jb] = (uint16_t)ib;                               // c_j
+                if (jb > 0) c16[2 * (jb - 1) + 1] = (uint16_t)(ib - lr);  // d_(j-1)
+            }
+            ib -= lr;
+            jb -= lc;
+        }
+        gi -= __shfl_sync(kFull, sr, G - 1, G);
+        gj -= __shfl_sync(kFull, sc, G - 1, G);
+    }
+}
+
+// One walker move from slot c of lane lw on anti-diagonal kw (parity e) by
+// code b: diagonal keeps the slot, up (d + 1) / left (d - 1) move to slot
+// c + e / c + e - 1 of the other parity.  Branch-free (the walkers of a warp
+// take different moves).
+template <int C>
+__device__ __forceinline__ void walk_move(uint32_t b, int& kw, int& e, int& lw, int& c) {
+    const bool dg = b & 1u;
+    int cn = c + (dg ? 0 : (b ? e : e - 1));
+    kw -= dg ? 2 : 1;
+    e ^= dg ? 0 : 1;
+    const bool hi = cn >= C, lo = cn < 0;
+    cn += hi ? -C : (lo ? C : 0);
+    lw += hi ? 1 : (lo ? -1 : 0);
+    c = cn;
+}
+
+// Backtracking with the record in shared memory (DM 2): lane 0 of the group
+// walks the whole record into the move log, reading the three possible next
+// elements while it decodes the current one; then the group builds the runs.
+template <int C>
+__device__ __forceinline__ void walk_shared(const PairArgs& a, unsigned char* smem,
+                                            const uint32_t* drow, int64_t pr, int L, int K,
+                                            int G, int l, int gib, int e0, int porg, bool live) {
+    using DT = DirT<C>;
+    const DT* rec = (const DT*)drow;
+    uint8_t* mlog = smem + (size_t)(blockDim.x >> a.lgG) * a.recb + (size_t)gib * a.logb;
+    uint16_t* r16 = (uint16_t*)(a.rows + pr * L);  // [2i] = a_i, [2i+1] = b_i
+    uint16_t* c16 = (uint16_t*)(a.cols + pr * L);  // [2j] = c_j, [2j+1] = d_j
+    __syncwarp();  // the group's record is visible to its walker
+    int nm = 0;
+    if (l == 0 && live) {
+        r16[2 * (L - 1) + 1] = (uint16_t)(L - 1);
+        c16[2 * (L - 1) + 1] = (uint16_t)(L - 1);
+        int kw = K - 1, e = e0, lw = porg / C, c = porg - lw * C;
+        uint32_t cur = rec[(size_t)kw * G + lw];
+        // every move lowers kw, so at most K moves (the log holds K bytes)
+        while (kw >= 0 && (unsigned)lw < (unsigned)G) {
+            const int r1 = max(kw - 1, 0), r2 = max(kw - 2, 0);
+            const uint32_t n2 = rec[r2 * G + lw];
+            const uint32_t n1 = rec[r1 * G + lw];
+            const uint32_t n1m = rec[r1 * G + max(lw - 1, 0)];
+            const uint32_t n1p = rec[r1 * G + min(lw + 1, G - 1)];
+            const uint32_t b = (cur >> (2 * c)) & 3u;
+            mlog[nm++] = (uint8_t)b;
+            const int lw0 = lw;
+            walk_move<C>(b, kw, e, lw, c);
+            cur = (b & 1u) ? n2 : (lw > lw0 ? n1p : (lw < lw0 ? n1m : n1));
+        }
+    }
+    nm = __shfl_sync(kFull, nm, 0, G);
+    const int nmax = __reduce_max_sync(kFull, (unsigned)nm);
+    __syncwarp();
+    int gi = L - 1, gj = L - 1;
+    runs_from_moves<4>(mlog, nm, nmax, G, l, live, L, r16, c16, gi, gj);
+}
+
+// Backtracking with the record in global scratch (DM 1): the record streams
+// into a kWalkStages-deep shared-memory ring in chunks of R anti-diagonals
+// (kWalkChunk bytes per lane, 16-byte cp.async copies), last chunk first;
+// lane 0 of the group decodes a chunk's moves into a byte log (2-bit codes: 1
+// or 3 diagonal, 2 up (i-1, j), 0 left (i, j-1)) and the group turns the log
+// into runs.  Cell (0, 0) always records a diagonal move (its diagonal is the
+// origin, the other predecessors are +inf): it writes the last runs and ends
+// the walk.
+template <int C>
+__device__ __forceinline__ void walk_ring(const PairArgs& a, unsigned char* smem,
+                                          const uint32_t* drow, int64_t pr, int L, int K, int G,
+                                          int l, int gib, int e0, int porg, bool live) {
+    using DT = DirT<C>;
+    constexpr int R = kWalkChunk / (int)sizeof(DT);  // anti-diagonals per chunk
+    unsigned char* ring = smem + (size_t)gib * kWalkStages * kWalkChunk * G;
+    uint8_t* mlog = smem + (size_t)blockDim.x * kWalkStages * kWalkChunk + gib * kMoveLog;
+    const int nch = (K + R - 1) / R;  // the record holds nch whole chunks per pair
+    const unsigned char* rec = (const unsigned char*)drow;
+    auto issue = [&](int ch) {
+        if (ch < nch) {
+            unsigned char* dst = ring + (ch % kWalkStages) * kWalkChunk * G;
+            const unsigned char* src = rec + (size_t)(nch - 1 - ch) * kWalkChunk * G;
+#pragma unroll 4
+            for (int t = l; t < kWalkChunk / 16 * G; t += G) cp_async16(dst + 16 * t, src + 16 * t);
+        }
+        cp_async_commit();
+    };
+    __syncwarp();  // the group's direction elements are visible to all its lanes
+#pragma unroll
+    for (int ch = 0; ch < kWalkStages - 1; ++ch) issue(ch);
+    uint16_t* r16 = (uint16_t*)(a.rows + pr * L);  // [2i] = a_i, [2i+1] = b_i
+    uint16_t* c16 = (uint16_t*)(a.cols + pr * L);  // [2j] = c_j, [2j+1] = d_j
+    if (l == 0 && live) {
+        r16[2 * (L - 1) + 1] = (uint16_t)(L - 1);
+        c16[2 * (L - 1) + 1] = (uint16_t)(L - 1);
+    }
+    int kw = K - 1, e = e0;                  // walker: anti-diagonal and its parity
+    int lw = porg / C, c = porg - lw * C;    // slot c of lane lw
+    int gi = L - 1, gj = L - 1;  // (group-uniform) cell before the chunk's first move
+    for (int ch = 0; ch < nch; ++ch) {  // same trip count in every group of the warp
+        issue(ch + kWalkStages - 1);
+        cp_async_wait<kWalkStages - 1>();
+        __syncwarp();
+        int nm = 0;
+        if (l == 0 && live) {  // groups past the last pair do not walk
+            const DT* buf = (const DT*)(ring + (ch % kWalkStages) * kWalkChunk * G);
+            const int rlo = (nch - 1 - ch) * R;
+            // every move lowers kw: at most R (<= kMoveLog) moves per chunk
+            while (kw >= rlo && (unsigned)lw < (unsigned)G) {
+                const uint32_t b = ((uint32_t)buf[(kw - rlo) * G + lw] >> (2 * c)) & 3u;
+                mlog[nm++] = (uint8_t)b;
+                walk_move<C>(b, kw, e, lw, c);
+            }
+        }
+        nm = __shfl_sync(kFull, nm, 0, G);
+        // every lane of the warp runs the same number of scan rounds (the
+        // groups' move counts differ): the full-mask shuffles below need it
+        const int nmax = __reduce_max_sync(kFull, (unsigned)nm);
+        __syncwarp();
+        runs_from_moves<1>(mlog, nm, nmax, G, l, live, L, r16, c16, gi, gj);
+        __syncwarp();
+    }
+    cp_async_wait<0>();
+}
+
+// DM: 0 distance only; 1 path record in global scratch, walked through a
+// shared-memory ring; 2 path record in shared memory (short pairs, C <= 4).
+template <int C, bool EU, int DM>
 __global__ void __launch_bounds__(kPairThreads, 4) pair_fwd_kernel(const PairArgs a) {
+    constexpr bool DIRS = DM != 0;
     extern __shared__ __align__(16) unsigned char smem[];
     const int G = a.G, L = a.L, W = a.W;
     const int tid = threadIdx.x;
@@ -223,22 +402,22 @@ __global__ void __launch_bounds__(kPairThreads, 4) pair_fwd_kernel(const PairArg
         st.Sv[c] = (j >= 0 && j < L) ? __ldg(ss + j) : 0.f;
     }
     st.bits = 0;
-    st.u = 0;
-    st.kb = 0;
     st.iq = (W - e0) / 2;                      // lane 0's slot-0 query index at k = 0
     st.js = (-W + 2 * (G * C - 1) + e0) / 2;  // lane G-1's last-slot subject index
     st.pq = (st.iq + 1 < L) ? __ldg(sq + st.iq + 1) : 0.f;
     st.ps = (st.js + 1 < L) ? __ldg(ss + st.js + 1) : 0.f;
-    uint32_t* drow = DIRS ? a.dirs + (size_t)pr * a.nkb * G : nullptr;
+    uint32_t* drow = DM == 1   ? a.dirs + (size_t)pr * a.dstride
+                     : DM == 2 ? (uint32_t*)(smem + (size_t)gib * a.recb)
+                               : nullptr;
 
     int k = 0;
     if (e0 == 0) {
         step_even<C, EU, DIRS, 0, 0>(st, sq, L, G, l, false);
-        flush_bits<C, DIRS>(st, drow, G, l, k, K, live);
+        store_dirs<C, DM>(st, drow, G, l, k, live);
         k = 1;
     } else {
         step_odd<C, EU, DIRS, 0, 0>(st, ss, L, G, l, false);
-        flush_bits<C, DIRS>(st, drow, G, l, k, K, live);
+        store_dirs<C, DM>(st, drow, G, l, k, live);
         k = 1;
         if (k < K) {
             // query shift with the rotation kept at 0: move the window down
@@ -251,11 +430,12 @@ __global__ void __launch_bounds__(kPairThreads, 4) pair_fwd_kernel(const PairArg
                 st.pq = st.iq + 1 < L ? __ldg(sq + st.iq + 1) : 0.f;
             }
             step_even<C, EU, DIRS, 0, 0>(st, sq, L, G, l, false);
-            flush_bits<C, DIRS>(st, drow, G, l, k, K, live);
+            store_dirs<C, DM>(st, drow, G, l, k, live);
             k = 2;
         }
     }
-    while (k < K) body<C, EU, DIRS, 0>(st, sq, ss, drow, L, G, l, k, K, live);
+    while (k + 2 * C <= K) body<C, EU, DM, false, 0>(st, sq, ss, drow, L, G, l, k, K, live);
+    if (k < K) body<C, EU, DM, true, 0>(st, sq, ss, drow, L, G, l, k, K, live);
 
     // D[L-1][L-1]: slot porg of the last anti-diagonal (parity e0)
     float dval = CDTW_INF;
@@ -263,113 +443,11 @@ __global__ void __launch_bounds__(kPairThreads, 4) pair_fwd_kernel(const PairArg
     for (int c = 0; c < C; ++c)
         if (p0 + c == porg) dval = (e0 == 0) ? st.A[c] : st.B[c];
     if (live && p0 <= porg && porg < p0 + C) a.D[pr] = dval;
-    if (!DIRS) return;
-
-    // Backtracking: chunks of kWalkRows direction rows stream into a
-    // kWalkStages-deep shared-memory ring (cp.async).  Lane 0 of the group
-    // decodes the moves of a chunk into a byte log (2-bit codes: 1 or 3
-    // diagonal, 2 up (i-1, j), 0 left (i, j-1)); the group then turns the log
-    // into row runs (a_i, b_i) and column runs (c_j, d_j) with a scan.  Cell
-    // (0, 0) always records a diagonal move (its diagonal is the origin, the
-    // other predecessors are +inf): it writes the last runs and ends the walk.
-    constexpr int S = 16 / C;
-    uint32_t* ring = (uint32_t*)smem + (size_t)gib * kWalkStages * kWalkRows * G;
-    uint8_t* mlog = smem + (size_t)blockDim.x * kWalkStages * kWalkRows * 4 + gib * kMoveLog;
-    const int nch = (a.nkb + kWalkRows - 1) / kWalkRows;
-    auto issue = [&](int ch) {
-        if (ch < nch) {
-            uint32_t* dst = ring + (ch % kWalkStages) * kWalkRows * G;
-            const int rhi = a.nkb - 1 - ch * kWalkRows;
-#pragma unroll 4
-            for (int t = 0; t < kWalkRows; ++t) {
-                const int r = rhi - t;
-                if (r >= 0) cp_async4(dst + t * G + l, drow + (size_t)r * G + l);
-            }
-        }
-        cp_async_commit();
-    };
-    __syncwarp();  // the group's direction words are visible to all its lanes
-#pragma unroll
-    for (int ch = 0; ch < kWalkStages - 1; ++ch) issue(ch);
-    uint16_t* r16 = (uint16_t*)(a.rows + pr * L);  // [2i] = a_i, [2i+1] = b_i
-    uint16_t* c16 = (uint16_t*)(a.cols + pr * L);  // [2j] = c_j, [2j+1] = d_j
-    if (l == 0 && live) {
-        r16[2 * (L - 1) + 1] = (uint16_t)(L - 1);
-        c16[2 * (L - 1) + 1] = (uint16_t)(L - 1);
+    if constexpr (DM == 1) {
+        walk_ring<C>(a, smem, drow, pr, L, K, G, l, gib, e0, porg, live);
+    } else if constexpr (DM == 2) {
+        walk_shared<C>(a, smem, drow, pr, L, K, G, l, gib, e0, porg, live);
     }
-    int kb = (K - 1) / S, uu = (K - 1) - kb * S, e = e0;  // walker: anti-diagonal kb*S+uu
-    int lw = porg / C, c = porg - lw * C;                  // slot c of lane lw, parity e
-    int gi = L - 1, gj = L - 1;  // (group-uniform) cell before the chunk's first move
-    for (int ch = 0; ch < nch; ++ch) {  // same trip count in every group of the warp
-        issue(ch + kWalkStages - 1);
-        cp_async_wait<kWalkStages - 1>();
-        __syncwarp();
-        int nm = 0;
-        if (l == 0 && live) {  // groups past the last pair do not walk
-            const uint32_t* buf = ring + (ch % kWalkStages) * kWalkRows * G;
-            const int rhi = a.nkb - 1 - ch * kWalkRows;
-            const int rlo = max(rhi - kWalkRows + 1, 0);
-            while (kb >= rlo && (unsigned)lw < (unsigned)G && nm < kMoveLog) {
-                const uint32_t wd = buf[(rhi - kb) * G + lw];
-                const uint32_t b = (wd >> (2 * C * (S - 1 - uu) + 2 * c)) & 3u;
-                mlog[nm++] = (uint8_t)b;
-                const bool dg = b & 1u;
-                const int dp = dg ? 0 : (b ? e : e - 1);  // up: d + 1, left: d - 1
-                e ^= dg ? 0 : 1;
-                if (S == 1) {
-                    kb -= 1 + dg;
-                } else {
-                    uu -= 1 + dg;
-                    if (uu < 0) {
-                        uu += S;
-                        --kb;
-                    }
-                }
-                c += dp;
-                if (c >= C) {
-                    c -= C;
-                    ++lw;
-                } else if (c < 0) {
-                    c += C;
-                    --lw;
-                }
-            }
-        }
-        nm = __shfl_sync(kFull, nm, 0, G);
-        // every lane of the warp runs the same number of scan rounds (the
-        // groups' move counts differ): the full-mask shuffles below need it
-        const int nmax = __reduce_max_sync(kFull, (unsigned)nm);
-        __syncwarp();
-        for (int m0 = 0; m0 < nmax; m0 += G) {
-            const int m = m0 + l;
-            const uint32_t b = m < nm ? mlog[m] : 2u;
-            const int lr = (m < nm && b != 0u) ? 1 : 0;  // leaves its row
-            const int lc = (m < nm && b != 2u) ? 1 : 0;  // leaves its column
-            int sr = lr, sc = lc;                        // inclusive scans over the group
-            for (int o = 1; o < G; o <<= 1) {
-                const int tr = __shfl_up_sync(kFull, sr, o, G);
-                const int tc = __shfl_up_sync(kFull, sc, o, G);
-                if (l >= o) {
-                    sr += tr;
-                    sc += tc;
-                }
-            }
-            const int ib = gi - (sr - lr), jb = gj - (sc - lc);  // cell before move m
-            const bool inside = live && (unsigned)ib < (unsigned)L && (unsigned)jb < (unsigned)L;
-            if (inside && lr) {
-                r16[2 * ib] = (uint16_t)jb;                               // a_i
-                if (ib > 0) r16[2 * (ib - 1) + 1] = (uint16_t)(jb - lc);  // b_(i-1)
-            }
-            if (inside && lc) {
-                c16[2 * jb] = (uint16_t)ib;                               // c_j
-                if (jb > 0) c16[2 * (jb - 1) + 1] = (uint16_t)(ib - lr);  // d_(j-1)
-            }
-            gi -= __shfl_sync(kFull, sr, G - 1, G);
-            gj -= __shfl_sync(kFull, sc, G - 1, G);
-        }
-        __syncwarp();
-    }
-    cp_async_wait<0>();
 }
 
 // z-normalisation of every series of the pairs: one warp per series, FP64
@@ -589,30 +667,35 @@ pair_bwd_kernel(const float* __restrict__ q, const float* __restrict__ s, int64_
 
 using PairFwdK = void (*)(const PairArgs);
 
+// dm 2 (shared record) is instantiated for C <= 4 only: the host selects it
+// for records of at most 512 bytes per lane, which needs C <= 4.
 template <int C>
-PairFwdK pick_fwd(bool eu, bool dirs) {
-    if (eu) return dirs ? pair_fwd_kernel<C, true, true> : pair_fwd_kernel<C, true, false>;
-    return dirs ? pair_fwd_kernel<C, false, true> : pair_fwd_kernel<C, false, false>;
+PairFwdK pick_fwd(bool eu, int dm) {
+    if constexpr (C <= 4) {
+        if (dm == 2) return eu ? pair_fwd_kernel<C, true, 2> : pair_fwd_kernel<C, false, 2>;
+    }
+    if (eu) return dm ? pair_fwd_kernel<C, true, 1> : pair_fwd_kernel<C, true, 0>;
+    return dm ? pair_fwd_kernel<C, false, 1> : pair_fwd_kernel<C, false, 0>;
 }
 
-PairFwdK fwd_kernel(int C, bool eu, bool dirs) {
+PairFwdK fwd_kernel(int C, bool eu, int dm) {
     switch (C) {
-        case 1: return pick_fwd<1>(eu, dirs);
-        case 2: return pick_fwd<2>(eu, dirs);
-        case 3: return pick_fwd<3>(eu, dirs);
-        case 4: return pick_fwd<4>(eu, dirs);
-        case 5: return pick_fwd<5>(eu, dirs);
-        case 6: return pick_fwd<6>(eu, dirs);
-        case 7: return pick_fwd<7>(eu, dirs);
-        case 8: return pick_fwd<8>(eu, dirs);
-        case 9: return pick_fwd<9>(eu, dirs);
-        case 10: return pick_fwd<10>(eu, dirs);
-        case 11: return pick_fwd<11>(eu, dirs);
-        case 12: return pick_fwd<12>(eu, dirs);
-        case 13: return pick_fwd<13>(eu, dirs);
-        case 14: return pick_fwd<14>(eu, dirs);
-        case 15: return pick_fwd<15>(eu, dirs);
-        default: return pick_fwd<16>(eu, dirs);
+        case 1: return pick_fwd<1>(eu, dm);
+        case 2: return pick_fwd<2>(eu, dm);
+        case 3: return pick_fwd<3>(eu, dm);
+        case 4: return pick_fwd<4>(eu, dm);
+        case 5: return pick_fwd<5>(eu, dm);
+        case 6: return pick_fwd<6>(eu, dm);
+        case 7: return pick_fwd<7>(eu, dm);
+        case 8: return pick_fwd<8>(eu, dm);
+        case 9: return pick_fwd<9>(eu, dm);
+        case 10: return pick_fwd<10>(eu, dm);
+        case 11: return pick_fwd<11>(eu, dm);
+        case 12: return pick_fwd<12>(eu, dm);
+        case 13: return pick_fwd<13>(eu, dm);
+        case 14: return pick_fwd<14>(eu, dm);
+        case 15: return pick_fwd<15>(eu, dm);
+        default: return pick_fwd<16>(eu, dm);
     }
 }
 
@@ -629,12 +712,14 @@ void pair_shape(int L, int W, int* G, int* C) {
     *C = (slots + g - 1) / g;
 }
 
+// Words of direction record per pair: whole backtracking chunks of R
+// anti-diagonals x G lane elements.
 size_t pair_dirs_words(int L, int W) {
     int G, C;
     pair_shape(L, W, &G, &C);
-    const int S = 16 / C;
-    const int64_t nkb = div_up(2 * (int64_t)L - 1, S);
-    return (size_t)nkb * G;
+    const int eb = C <= 4 ? 1 : (C <= 8 ? 2 : 4);
+    const int64_t nch = div_up(2 * (int64_t)L - 1, kWalkChunk / eb);
+    return (size_t)(nch * kWalkChunk * G / 4);
 }
 
 int launch_pair_znorm(cdtw_handle h, const float* q, const float* s, int64_t n, int L, float* zq,
@@ -662,17 +747,27 @@ int launch_pair_fwd(cdtw_handle h, const float* zq, const float* zs, int64_t n, 
     while ((1 << a.lgG) < G) ++a.lgG;
     a.D = D;
     a.dirs = dirs;
-    a.nkb = (int)div_up(2 * (int64_t)L - 1, 16 / C);
+    a.dstride = (int)pair_dirs_words(L, W);
     a.rows = rows;
     a.cols = cols;
     const int threads = kPairThreads;
-    // backtracking ring (kWalkStages x kWalkRows words per lane) + move log per group
-    const size_t smem =
-        dirs ? (size_t)threads * kWalkStages * kWalkRows * 4 + (size_t)(threads / G) * kMoveLog : 0;
     const int64_t groups_per_block = threads / G;
+    // path record in shared memory when it takes at most 512 bytes per lane
+    // and the block's records and move logs leave room for 3 blocks per SM
+    const int K = 2 * L - 1;
+    a.recb = (int)round_up((int64_t)K * G, 16);  // one byte per lane and anti-diagonal (C <= 4)
+    a.logb = (int)round_up(K, 16);
+    const size_t shared_rec = (size_t)groups_per_block * (a.recb + a.logb);
+    const int dm = !dirs ? 0 : (C <= 4 && K <= 512 && shared_rec <= kSharedRecMax) ? 2 : 1;
+    // DM 1: backtracking ring (kWalkStages chunks of kWalkChunk bytes per lane)
+    // + move log per group
+    const size_t smem =
+        dm == 2   ? shared_rec
+        : dm == 1 ? (size_t)threads * kWalkStages * kWalkChunk + (size_t)groups_per_block * kMoveLog
+                  : 0;
     const int64_t blocks = div_up(n, groups_per_block);
     if (blocks > INT32_MAX) return set_error(h, CDTW_EINVAL, "too many pairs");
-    const PairFwdK k = fwd_kernel(C, euclid, dirs != nullptr);
+    const PairFwdK k = fwd_kernel(C, euclid, dm);
     CDTW_CUDA(h, cudaFuncSetAttribute((const void*)k, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)smem));
     k<<<(int)blocks, threads, smem, h->stream>>>(a);
