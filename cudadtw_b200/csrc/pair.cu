@@ -755,8 +755,10 @@ int launch_pair_fwd(cdtw_handle h, const float* zq, const float* zs, int64_t n, 
     // path record in shared memory when it takes at most 512 bytes per lane
     // and the block's records and move logs leave room for 3 blocks per SM
     const int K = 2 * L - 1;
-    a.recb = (int)round_up((int64_t)K * G, 16);  // one byte per lane and anti-diagonal (C <= 4)
-    a.logb = (int)round_up(K, 16);
+    // one byte per lane and anti-diagonal (C <= 4); strides of 32 (mod 128)
+    // bytes put the groups of a warp on different shared-memory banks
+    a.recb = (int)round_up((int64_t)K * G, 128) + 32;
+    a.logb = (int)round_up(K, 128) + 32;
     const size_t shared_rec = (size_t)groups_per_block * (a.recb + a.logb);
     const int dm = !dirs ? 0 : (C <= 4 && K <= 512 && shared_rec <= kSharedRecMax) ? 2 : 1;
     // DM 1: backtracking ring (kWalkStages chunks of kWalkChunk bytes per lane)
