@@ -283,7 +283,14 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
                         "d2h_bytes_per_step": len(bands) * nw * 4},
                 "roofline": {"bound": "alu", "kernel": "cdtw_reg2_kernel",
                              "achieved": ach, "peak": peak / 1e9, "unit": "GCUPS",
-                             "frac": ach / (peak / 1e9), "traffic": None,
+                             "frac": ach / (peak / 1e9),
+                             # DRAM bytes (read + write) of one cdtw_reg2_kernel launch
+                             # of this workload from an ncu capture (both bands 69.2 MB:
+                             # stream, window statistics, results); not measured here
+                             "traffic": 69.2e6, "traffic_unit": "bytes per launch",
+                             "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write"
+                                               ".sum, profiles/cdtw_reg2_kernel_raw_allwindows"
+                                               "_m128_n4M.md",
                              "per_band": {str(w): a for w, a in zip(bands, achieved)},
                              "peak_source": "measured: cdtw_calibrate_cell_rate (FADD+FMNMX3+FFMA"
                                             " chains) on this GPU in this run"},
