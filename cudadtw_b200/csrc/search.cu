@@ -223,6 +223,33 @@ size_t topk_workspace_bytes(int64_t N, int M) {
     return carve_topk(N, Nw, M, topk_cap(Nw), &sw, &tw, nullptr);
 }
 
+// Greedy non-overlapping selection over the (distance, window) keys in
+// ascending order: a window overlapping an accepted one is skipped, and the
+// selection stops at k.  The keys are unique; only the prefix the greedy
+// consumes is ordered: nth_element splits off the next smallest block, which
+// is sorted and scanned, the block doubling until k windows are accepted.
+static void greedy_picks(std::vector<unsigned long long>& hits, int k, int M,
+                         std::vector<unsigned long long>* picks) {
+    std::set<int64_t> taken;
+    picks->clear();
+    size_t lo = 0, block = std::max<size_t>(4096, (size_t)16 * (size_t)k);
+    while (lo < hits.size() && (int)picks->size() < k) {
+        const size_t hi = std::min(hits.size(), lo + block);
+        if (hi < hits.size()) std::nth_element(hits.begin() + lo, hits.begin() + hi, hits.end());
+        std::sort(hits.begin() + lo, hits.begin() + hi);
+        for (size_t i = lo; i < hi && (int)picks->size() < k; ++i) {
+            const unsigned long long key = hits[i];
+            const int64_t w = (int64_t)(uint32_t)key;
+            auto it = taken.lower_bound(w - M + 1);
+            if (it != taken.end() && *it < w + M) continue;  // overlaps an accepted window
+            taken.insert(w);
+            picks->push_back(key);
+        }
+        lo = hi;
+        block *= 2;
+    }
+}
+
 // Top-k non-overlapping matches of the handle's query.  Greedy selection in
 // (distance, window) order with windows overlapping an accepted one skipped.
 // The candidate threshold T is the 2k-th smallest cDTW among the segment
@@ -301,17 +328,7 @@ int run_topk(cdtw_handle h, const float* x, int64_t N, const double* mu, const f
         CDTW_CUDA(h, cudaStreamSynchronize(h->stream));
     }
     // 4. greedy non-overlapping selection, lowest (distance, window) first
-    std::sort(hits.begin(), hits.end());
-    std::set<int64_t> taken;
-    picks->clear();
-    for (const unsigned long long key : hits) {
-        if ((int)picks->size() >= k) break;
-        const int64_t w = (int64_t)(uint32_t)key;
-        auto it = taken.lower_bound(w - M + 1);
-        if (it != taken.end() && *it < w + M) continue;  // overlaps an accepted window
-        taken.insert(w);
-        picks->push_back(key);
-    }
+    greedy_picks(hits, k, M, picks);
     return CDTW_OK;
 }
 
