@@ -136,6 +136,7 @@ batch_seed_kernel(const BatchArgs b) {
         __syncthreads();
         for (int base = (tid & ~31); base < Tq; base += kBatchThreads) {
             const int l = base + lane;
+            float lb = CDTW_INF;
             if (l < Tq) {
                 const Norm nm = make_norm(ts.mu[l], ts.sg[l]);
                 float sv[10], qv[10];
@@ -146,9 +147,11 @@ batch_seed_kernel(const BatchArgs b) {
                     sv[5 + k] = znorm(nm, ts.xs[l + M - 5 + k]);
                     qv[5 + k] = __ldg(Q.zq + M - 5 + k);
                 }
-                const float lb = lb_kim_dp<EU>(sv, qv);
-                if (lb == lb) atomicMin(&s_best, pack_key(lb, (uint32_t)l));
+                lb = lb_kim_dp<EU>(sv, qv);
             }
+            // base is warp-uniform: every lane of the warp is here
+            const unsigned long long k = warp_min_key(l < Tq && lb == lb, lb, (uint32_t)l);
+            if (lane == 0 && k != ~0ull) atomicMin(&s_best, k);  // one per warp
         }
         __syncthreads();
         if (tid == 0) {

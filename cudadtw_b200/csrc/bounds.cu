@@ -60,7 +60,9 @@ lb_kim_kernel(const float* __restrict__ x, const double* __restrict__ mu,
         out[t] = v;
     }
     if (seeds) {  // the block's smallest bound: a seed window for the search
-        if (t < L && w >= 0 && w < Nw && v == v) atomicMin(&best, pack_key(v, (uint32_t)w));
+        const unsigned long long k =
+            warp_min_key(t < L && w >= 0 && w < Nw && v == v, v, (uint32_t)w);
+        if ((threadIdx.x & 31) == 0 && k != ~0ull) atomicMin(&best, k);  // one per warp
         __syncthreads();
         if (threadIdx.x == 0) seeds[blockIdx.x] = best;
     }

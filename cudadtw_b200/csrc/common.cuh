@@ -207,6 +207,17 @@ __host__ __device__ inline unsigned long long pack_key(float d, uint32_t idx) {
 #endif
 }
 
+// Smallest packed (distance, index) key over the lanes of a warp: the least
+// distance bits, then the lowest index among the lanes holding them; equal to
+// the minimum of pack_key over the lanes with ok set (distances >= 0), ~0 when
+// no lane has it.  All 32 lanes call.
+__device__ __forceinline__ unsigned long long warp_min_key(bool ok, float d, uint32_t idx) {
+    const unsigned db = ok ? __float_as_uint(d) : 0xffffffffu;
+    const unsigned dmin = __reduce_min_sync(0xffffffffu, db);
+    const unsigned im = __reduce_min_sync(0xffffffffu, (ok && db == dmin) ? idx : 0xffffffffu);
+    return ((unsigned long long)dmin << 32) | im;
+}
+
 // A search candidate: window, its best lower bound, and its forward LB_Keogh
 // (the sum whose suffixes give the cumulative bound for early abandoning).
 struct Cand {
