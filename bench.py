@@ -438,9 +438,11 @@ def subresults(h, dev) -> dict:
         c = cells(L, W)
         r["fwd_gcups"] = n * c / (r["fwd_ms"] / 1e3) / 1e9
         r["fwd_bwd_over_fwd"] = r["fwd_bwd_ms"] / r["fwd_ms"]
+        scratch = h.pair_workspace_bytes(1, L, W, False, True)
         r["bytes_per_pair"] = {"path_record": h.pair_path_bytes(1, L),
-                               "direction_scratch": h.pair_workspace_bytes(1, L, W, False, True),
+                               "direction_scratch": scratch,
                                "full_fp32_band_table": 4 * c}
+        r["direction_record_in"] = "shared memory" if scratch == 0 else "device scratch"
         pair[f"{n}x{L}_W{W}"] = r
         del q, s, path, gq, gs
     out["pair_fwd_bwd"] = pair

@@ -712,11 +712,27 @@ void pair_shape(int L, int W, int* G, int* C) {
     *C = (slots + g - 1) / g;
 }
 
-// Words of direction record per pair: whole backtracking chunks of R
-// anti-diagonals x G lane elements.
+// Shared-record mode of the forward with a path: the record stays in shared
+// memory when it takes at most 512 bytes per lane (C <= 4, one byte per lane
+// and anti-diagonal) and the block's records and move logs leave room for 3
+// blocks per SM.  recb / logb: bytes per group, with strides of 32 (mod 128)
+// bytes so the groups of a warp sit on different shared-memory banks.
+static bool pair_shared_record(int L, int G, int C, int* recb, int* logb, size_t* bytes) {
+    const int K = 2 * L - 1;
+    *recb = (int)round_up((int64_t)K * G, 128) + 32;
+    *logb = (int)round_up(K, 128) + 32;
+    *bytes = (size_t)(kPairThreads / G) * (size_t)(*recb + *logb);
+    return C <= 4 && K <= 512 && *bytes <= kSharedRecMax;
+}
+
+// Words of direction record per pair in device scratch: whole backtracking
+// chunks of R anti-diagonals x G lane elements; 0 in shared-record mode.
 size_t pair_dirs_words(int L, int W) {
     int G, C;
     pair_shape(L, W, &G, &C);
+    int recb, logb;
+    size_t shared_bytes;
+    if (pair_shared_record(L, G, C, &recb, &logb, &shared_bytes)) return 0;
     const int eb = C <= 4 ? 1 : (C <= 8 ? 2 : 4);
     const int64_t nch = div_up(2 * (int64_t)L - 1, kWalkChunk / eb);
     return (size_t)(nch * kWalkChunk * G / 4);
@@ -752,15 +768,13 @@ int launch_pair_fwd(cdtw_handle h, const float* zq, const float* zs, int64_t n, 
     a.cols = cols;
     const int threads = kPairThreads;
     const int64_t groups_per_block = threads / G;
-    // path record in shared memory when it takes at most 512 bytes per lane
-    // and the block's records and move logs leave room for 3 blocks per SM
-    const int K = 2 * L - 1;
-    // one byte per lane and anti-diagonal (C <= 4); strides of 32 (mod 128)
-    // bytes put the groups of a warp on different shared-memory banks
-    a.recb = (int)round_up((int64_t)K * G, 128) + 32;
-    a.logb = (int)round_up(K, 128) + 32;
-    const size_t shared_rec = (size_t)groups_per_block * (a.recb + a.logb);
-    const int dm = !dirs ? 0 : (C <= 4 && K <= 512 && shared_rec <= kSharedRecMax) ? 2 : 1;
+    // a path is recorded when the run arrays are given; the direction scratch
+    // is needed only outside shared-record mode
+    size_t shared_rec;
+    const bool shared = pair_shared_record(L, G, C, &a.recb, &a.logb, &shared_rec);
+    const int dm = !rows ? 0 : shared ? 2 : 1;
+    if (dm != 0 && !cols) return set_error(h, CDTW_EINVAL, "path record without column runs");
+    if (dm == 1 && !dirs) return set_error(h, CDTW_EINVAL, "path record without direction scratch");
     // DM 1: backtracking ring (kWalkStages chunks of kWalkChunk bytes per lane)
     // + move log per group
     const size_t smem =

@@ -29,6 +29,23 @@ def test_status_strings_and_null_handle():
     assert lib.cdtw_create(None, 0) == 1
 
 
+def test_pair_sizes():
+    """Path record and direction scratch sizes (host-only sizing calls)."""
+    lib = _lib.load()
+    # path record: 4 doubles + row and column runs (2 x L words) per pair
+    for L in (1, 256, 2048):
+        assert lib.cdtw_pair_path_bytes(3, L) == 3 * (32 + 8 * L)
+    # short pairs keep the direction record in shared memory: only the
+    # z-normalised copies (2 x n x L floats, 256-byte slices) are scratch
+    assert lib.cdtw_pair_workspace_bytes(1, 256, 25, 0, 1) == 0
+    assert lib.cdtw_pair_workspace_bytes(4096, 256, 25, 1, 1) == 2 * 4096 * 256 * 4
+    # long pairs: 2 bits per band cell in whole 64-byte-per-lane chunks of
+    # 16 anti-diagonals (32 lanes of 13 slots, 32-bit elements)
+    assert lib.cdtw_pair_workspace_bytes(1, 2048, 409, 0, 1) == 256 * 64 * 32
+    assert lib.cdtw_pair_workspace_bytes(1, 2048, 409, 0, 0) == 0
+    assert lib.cdtw_pair_workspace_bytes(0, 256, 25, 0, 1) == 0  # invalid size
+
+
 def test_create_without_gpu_fails_cleanly():
     import torch
     if torch.cuda.is_available():
