@@ -184,12 +184,32 @@ __device__ __forceinline__ float reg_window_dtw(const float4* sq4, int lq4,
     for (int k = 0; k <= B; ++k) prev[k] = CDTW_INF;
     prev[W] = 0.0f;
     float res = CDTW_INF, pre = 0.f;
+    // W <= 64: the samples of the next 4-row group are loaded one group ahead
+    // (with few windows in flight their latency is not hidden by other warps;
+    // wider bands leave no registers for it)
+    constexpr bool kAhead = W <= 64;
+    float xn[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) xn[u] = kAhead ? __ldg(xw + min(u, M - 1)) : 0.f;
     for (int j0 = 0; j0 < M; j0 += 4) {
+        float xc[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            if constexpr (kAhead) {
+                xc[u] = xn[u];
+                xn[u] = __ldg(xw + min(j0 + 4 + u, M - 1));
+            } else {
+                xc[u] = __ldg(xw + min(j0 + u, M - 1));
+            }
+        }
+        const bool check = (j0 & 7) == 4 && j0 + 3 < M - 1;  // rows j0..j0+3 are all real rows
+        // W <= 64: the best-so-far is read before the group's cells
+        const float bsf_early = (kAhead && check) ? load_bsf(key) : 0.f;
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
             const int j = j0 + u;
             const int jc = min(j, M - 1);
-            const float z = znorm(nm, __ldg(xw + jc));
+            const float z = znorm(nm, xc[u]);
             // forward LB_Keogh term of this data row (query envelope at j)
             const float2 e = senv[jc];
             const float dl = max3f(z - e.y, e.x - z, 0.f);
@@ -216,11 +236,11 @@ __device__ __forceinline__ float reg_window_dtw(const float4* sq4, int lq4,
 #pragma unroll
             for (int k = 0; k < B; ++k) prev[k] = cur[k];
         }
-        if ((j0 & 7) == 4 && j0 + 3 < M - 1) {  // rows j0..j0+3 are all real rows
+        if (check) {
             float rmin = prev[0];
 #pragma unroll
             for (int k = 1; k < B; k += 2) rmin = min3f(rmin, prev[k], prev[k + 1]);
-            alive = alive && (rmin + (lbk - pre) * kLbSlack < load_bsf(key));
+            alive = alive && (rmin + (lbk - pre) * kLbSlack < (kAhead ? bsf_early : load_bsf(key)));
             if (!__any_sync(0xffffffffu, alive)) return CDTW_INF;
         }
     }
