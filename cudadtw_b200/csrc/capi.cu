@@ -105,6 +105,8 @@ static int finish_search(cdtw_handle h, const unsigned long long* key, const int
     h->last_counts[1] = c[0];
     h->last_counts[2] = c[1];
     if (k == ~0ull) return set_error(h, CDTW_ECUDA, "search produced no result");
+    if ((uint32_t)k == 0xffffffffu)  // only the seeds' upper bound: no window beat it
+        return set_error(h, CDTW_ECUDA, "search kept the seed bound, not a window");
     const uint32_t bits = (uint32_t)(k >> 32);
     float d;
     memcpy(&d, &bits, 4);

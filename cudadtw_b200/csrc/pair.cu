@@ -35,8 +35,9 @@ constexpr int kWalkChunk = 64;  // bytes of direction record per lane in one bac
 constexpr unsigned kFull = 0xffffffffu;
 
 struct PairArgs {
-    const float* zq;      // DP inputs: n x L (z-normalised copies or the raw series)
-    const float* zs;
+    const float* zq;      // DP inputs: n x L (z-normalised copies or the raw series);
+    const float* zs;      // pair p's query starts at zq + p * qstride (0: one shared query)
+    int64_t qstride;
     int64_t n;
     int L, W, G, lgG;
     float* D;             // n outputs
@@ -381,7 +382,7 @@ __global__ void __launch_bounds__(kPairThreads, 4) pair_fwd_kernel(const PairArg
     const int64_t grp = (int64_t)blockIdx.x * (blockDim.x >> a.lgG) + gib;
     const bool live = grp < a.n;
     const int64_t pr = live ? grp : a.n - 1;
-    const float* sq = a.zq + pr * L;  // the pair's series (L2-resident; edge lanes read them)
+    const float* sq = a.zq + pr * a.qstride;  // the pair's series (L2-resident; edge lanes read them)
     const float* ss = a.zs + pr * L;
 
     const int K = 2 * L - 1;
@@ -748,13 +749,15 @@ int launch_pair_znorm(cdtw_handle h, const float* q, const float* s, int64_t n, 
 }
 
 int launch_pair_fwd(cdtw_handle h, const float* zq, const float* zs, int64_t n, int L, int W,
-                    bool euclid, float* D, uint32_t* dirs, uint32_t* rows, uint32_t* cols) {
+                    bool euclid, float* D, uint32_t* dirs, uint32_t* rows, uint32_t* cols,
+                    int64_t qstride) {
     int G, C;
     pair_shape(L, W, &G, &C);
     if (C > 16) return set_error(h, CDTW_EUNSUPPORTED, "pair band W=%d exceeds 511", W);
     PairArgs a;
     a.zq = zq;
     a.zs = zs;
+    a.qstride = qstride < 0 ? L : qstride;
     a.n = n;
     a.L = L;
     a.W = W;

@@ -40,9 +40,46 @@ struct SearchWs {
     float* envscratch = nullptr;
     int* ctr = nullptr;  // [0] n1, [1] n2, [2] work seeds, [3] work main, [4] n seeds
     unsigned long long* key = nullptr;
+    float* seed_z = nullptr;  // z-normalised seed windows (seed_cap floats)
+    float* seed_d = nullptr;  // their cDTW (kSeedMax floats)
+    int64_t seed_cap = 0;
 };
 
 constexpr int kKimBlock = 256;
+constexpr int kSeedMax = 4096;                     // seed_target's upper limit
+constexpr int64_t kSeedZMax = (int64_t)1 << 24;    // floats of seed windows (64 MB)
+constexpr float kSeedBoundSlack = 1.0f + 1e-4f;
+
+// The seed windows, z-normalised (FP64 arithmetic, rounded once), one row of
+// M floats per seed: the subjects of the seeds' pairwise cDTW.  One warp per
+// seed.
+__global__ void seed_gather_kernel(const float* __restrict__ x, const double* __restrict__ mu,
+                                   const float* __restrict__ sigma, const Cand* __restrict__ cands,
+                                   int nseed, int M, float* __restrict__ z) {
+    const int lane = threadIdx.x & 31;
+    const int i = (int)(((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    if (i >= nseed) return;
+    const int w = cands[i].w;
+    const double m = mu[w], inv = 1.0 / (double)sigma[w];
+    float* zi = z + (int64_t)i * M;
+    for (int j = lane; j < M; j += 32) zi[j] = (float)(((double)__ldg(x + w + j) - m) * inv);
+}
+
+// First best-so-far from the seeds' cDTW: the smallest distance, raised by
+// kSeedBoundSlack relative and 1e-6 per query sample absolute, and paired with
+// no window (index 0xffffffff).  The seed z-values are rounded once from FP64,
+// the search kernels' differ by at most an ulp, so the seed window's own
+// distance as the search kernels compute it lies below this bound (also for
+// an exact match, distance 0): the bound prunes nothing that could be the
+// best, and the best window replaces it in the key.
+__global__ void seed_bound_kernel(const float* __restrict__ d, const Cand* __restrict__ cands,
+                                  int nseed, int M, unsigned long long* __restrict__ key) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool ok = i < nseed && cands[i].lb < CDTW_INF && d[i] == d[i] && d[i] < CDTW_INF;
+    const float b = ok ? d[i] * kSeedBoundSlack + 1e-6f * (float)M : CDTW_INF;
+    const unsigned long long k = warp_min_key(ok, b, 0xffffffffu);
+    if ((threadIdx.x & 31) == 0 && k != ~0ull) atomicMin(key, k);
+}
 
 // Seed candidates: the smallest LB_Kim window of each group of G blocks.
 __global__ void seeds_to_cands_kernel(const unsigned long long* __restrict__ seeds, int nblk,
@@ -132,7 +169,7 @@ keogh_filter_kernel(const float* __restrict__ x, const double* __restrict__ mu,
     }
 }
 
-size_t carve_search(int64_t N, int64_t Nw, SearchWs* ws, char* base) {
+size_t carve_search(int64_t N, int64_t Nw, int M, SearchWs* ws, char* base) {
     size_t off = 0;
     auto take = [&](size_t bytes) {
         const size_t o = off;
@@ -149,6 +186,9 @@ size_t carve_search(int64_t N, int64_t Nw, SearchWs* ws, char* base) {
     ws->envscratch = (float*)take(stream_envelope_scratch_bytes(N));
     ws->ctr = (int*)take(sizeof(int) * 8);
     ws->key = (unsigned long long*)take(sizeof(unsigned long long));
+    ws->seed_cap = std::min<int64_t>(std::min<int64_t>(nblk, kSeedMax) * M, kSeedZMax);
+    ws->seed_z = (float*)take(sizeof(float) * ws->seed_cap);
+    ws->seed_d = (float*)take(sizeof(float) * kSeedMax);
     return off;
 }
 
@@ -196,7 +236,7 @@ struct TopkWs {
 
 size_t carve_topk(int64_t N, int64_t Nw, int M, int64_t cap, SearchWs* sw, TopkWs* tw,
                   char* base) {
-    size_t off = carve_search(N, Nw, sw, base);
+    size_t off = carve_search(N, Nw, M, sw, base);
     auto take = [&](size_t bytes) {
         const size_t o = off;
         off = (size_t)round_up((int64_t)(off + bytes), 256);
@@ -334,7 +374,7 @@ int run_topk(cdtw_handle h, const float* x, int64_t N, const double* mu, const f
 
 size_t search_workspace_bytes(int64_t N, int M) {
     SearchWs ws;
-    return carve_search(N, N - M + 1, &ws, nullptr);
+    return carve_search(N, N - M + 1, M, &ws, nullptr);
 }
 
 // Runs the whole pruned search; the result key and the stage counts stay on
@@ -344,7 +384,7 @@ int run_search(cdtw_handle h, const float* x, int64_t N, const double* mu, const
     const QueryPack& q = h->q;
     const int64_t Nw = N - q.M + 1;
     SearchWs ws;
-    carve_search(N, Nw, &ws, ws_base);
+    carve_search(N, Nw, q.M, &ws, ws_base);
     CDTW_CUDA(h, cudaMemsetAsync(ws.ctr, 0, sizeof(int) * 8, h->stream));
     CDTW_CUDA(h, cudaMemsetAsync(ws.key, 0xff, sizeof(unsigned long long), h->stream));
     // 1. LB_Kim of every window + per-block seeds
@@ -356,8 +396,24 @@ int run_search(cdtw_handle h, const float* x, int64_t N, const double* mu, const
     seeds_to_cands_kernel<<<(unsigned)div_up(nseed, 256), 256, 0, h->stream>>>(
         ws.seeds, (int)nblk, G, ws.seed_cands, ws.ctr + 4);
     CDTW_LAUNCH(h, "seeds_to_cands_kernel");
-    CDTW_TRY(launch_cdtw_search(h, x, N, mu, sigma, ws.seed_cands, ws.ctr + 4, ws.ctr + 2,
-                                nseed, euclid, ws.key));
+    // the seeds only bound the search from above, so their cDTW runs as
+    // pairwise wavefronts (a lane group per seed: low latency with few
+    // windows in flight) when the band and the seed windows fit
+    const int Wp = std::min(q.W, q.M - 1);
+    if (Wp <= CDTW_PAIR_MAX_BAND && q.M <= CDTW_MAX_QUERY && nseed <= kSeedMax &&
+        (int64_t)nseed * q.M <= ws.seed_cap) {
+        seed_gather_kernel<<<(unsigned)div_up((int64_t)nseed * 32, 256), 256, 0, h->stream>>>(
+            x, mu, sigma, ws.seed_cands, nseed, q.M, ws.seed_z);
+        CDTW_LAUNCH(h, "seed_gather_kernel");
+        CDTW_TRY(launch_pair_fwd(h, q.zq, ws.seed_z, nseed, q.M, Wp, euclid, ws.seed_d, nullptr,
+                                 nullptr, nullptr, /*qstride=*/0));
+        seed_bound_kernel<<<(unsigned)div_up(nseed, 256), 256, 0, h->stream>>>(
+            ws.seed_d, ws.seed_cands, nseed, q.M, ws.key);
+        CDTW_LAUNCH(h, "seed_bound_kernel");
+    } else {
+        CDTW_TRY(launch_cdtw_search(h, x, N, mu, sigma, ws.seed_cands, ws.ctr + 4, ws.ctr + 2,
+                                    nseed, euclid, ws.key));
+    }
     // 3. compaction by LB_Kim
     const int grid = h->sm_count * 8;
     compact_kim_kernel<<<grid, 256, 0, h->stream>>>(ws.lbkim, (int)Nw, ws.key, ws.q1, ws.ctr + 0);

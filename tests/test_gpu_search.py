@@ -124,6 +124,23 @@ def test_search_host_path_and_ties(handle):
     assert loc == int(np.argmin(allw))  # lowest index among equal distances
 
 
+@pytest.mark.parametrize("m,w", [(128, 12), (300, 60), (512, 102), (96, 0)])
+def test_search_exact_match_beats_seed_bound(handle, m, w):
+    """A query equal to one of the windows (distance about 0).  The seeds'
+    pairwise cDTW gives the search only an upper bound (raised a little, with
+    no window); the exact window must replace it, for both metrics and for
+    register-band and strip bands."""
+    x = synth.metal_like(50000, seed=m + w)
+    q, off = synth.cut_query(x, m, seed=w + 3, noise=0.0)
+    for metric in (0, 1):
+        dx, avg, std = _prep(handle, q, x, w)
+        loc, dist = handle.prune_cdtw(dx, avg, std, metric=metric)
+        allw = handle.gpu_cdtw(dx, avg, std, metric=metric).cpu().numpy()
+        best = allw.min()
+        assert loc == int(np.argmin(allw)) and best < 1e-3
+        assert dist == np.float32(np.sqrt(best) if metric == 0 else best)
+
+
 def test_search_with_constant_windows(handle):
     x = synth.ecg_like(20000, seed=4)
     x[5000:7000] = 2.0  # zero-variance windows: sigma = 1 (stats.cuh:50)
