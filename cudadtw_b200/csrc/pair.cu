@@ -44,6 +44,8 @@ struct PairArgs {
     uint32_t* dirs;       // per pair dstride words: 2L-1 rows of G lane elements (path record)
     int dstride;
     int recb, logb;       // shared-record mode: bytes of record and move log per group
+    const int* gate;      // when set and *gate > gate_max the launch does nothing
+    int gate_max;
     uint32_t* rows;       // per pair L words: a_i | b_i << 16
     uint32_t* cols;       // per pair L words: c_j | d_j << 16
 };
@@ -375,6 +377,7 @@ template <int C, bool EU, int DM>
 __global__ void __launch_bounds__(kPairThreads, 4) pair_fwd_kernel(const PairArgs a) {
     constexpr bool DIRS = DM != 0;
     extern __shared__ __align__(16) unsigned char smem[];
+    if (a.gate && *a.gate > a.gate_max) return;  // uniform for the whole launch
     const int G = a.G, L = a.L, W = a.W;
     const int tid = threadIdx.x;
     const int l = tid & (G - 1);
@@ -750,7 +753,7 @@ int launch_pair_znorm(cdtw_handle h, const float* q, const float* s, int64_t n, 
 
 int launch_pair_fwd(cdtw_handle h, const float* zq, const float* zs, int64_t n, int L, int W,
                     bool euclid, float* D, uint32_t* dirs, uint32_t* rows, uint32_t* cols,
-                    int64_t qstride) {
+                    int64_t qstride, const int* gate, int gate_max) {
     int G, C;
     pair_shape(L, W, &G, &C);
     if (C > 16) return set_error(h, CDTW_EUNSUPPORTED, "pair band W=%d exceeds 511", W);
@@ -758,6 +761,8 @@ int launch_pair_fwd(cdtw_handle h, const float* zq, const float* zs, int64_t n, 
     a.zq = zq;
     a.zs = zs;
     a.qstride = qstride < 0 ? L : qstride;
+    a.gate = gate;
+    a.gate_max = gate_max;
     a.n = n;
     a.L = L;
     a.W = W;

@@ -49,6 +49,8 @@ constexpr int kKimBlock = 256;
 constexpr int kSeedMax = 4096;                     // seed_target's upper limit
 constexpr int64_t kSeedZMax = (int64_t)1 << 24;    // floats of seed windows (64 MB)
 constexpr float kSeedBoundSlack = 1.0f + 1e-4f;
+constexpr int kWaveSurvivors = 512;                // survivors cDTW'd as wavefronts
+constexpr double kWaveMinCells = 4.0e4;            // band cells per window for that
 
 // The seed windows, z-normalised (FP64 arithmetic, rounded once), one row of
 // M floats per seed: the subjects of the seeds' pairwise cDTW.  One warp per
@@ -63,6 +65,41 @@ __global__ void seed_gather_kernel(const float* __restrict__ x, const double* __
     const double m = mu[w], inv = 1.0 / (double)sigma[w];
     float* zi = z + (int64_t)i * M;
     for (int j = lane; j < M; j += 32) zi[j] = (float)(((double)__ldg(x + w + j) - m) * inv);
+}
+
+// The survivors of the bounds when there are at most `cap`, z-normalised
+// exactly as the search kernels do (make_norm / znorm), for their pairwise
+// wavefront cDTW; rows past the survivor count repeat a valid window and are
+// ignored.  Thread 0 starts the search kernels' work counter at cap (they
+// then find nothing left), or at 0 when there are more survivors than cap
+// (the wavefront pass is skipped and they take all).
+__global__ void wave_gather_kernel(const float* __restrict__ x, const double* __restrict__ mu,
+                                   const float* __restrict__ sigma, const Cand* __restrict__ cands,
+                                   const int* __restrict__ count, int cap, int M,
+                                   float* __restrict__ z, int* __restrict__ work) {
+    const int lane = threadIdx.x & 31;
+    const int i = (int)(((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    const int n = *count;
+    if (blockIdx.x == 0 && threadIdx.x == 0) *work = n > cap ? 0 : cap;
+    if (i >= cap || n > cap) return;
+    const int w = i < n ? cands[i].w : (n > 0 ? cands[0].w : 0);
+    const Norm nm = make_norm(mu[w], sigma[w]);
+    float* zi = z + (int64_t)i * M;
+    for (int j = lane; j < M; j += 32) zi[j] = znorm(nm, __ldg(x + w + j));
+}
+
+// Exact keys of the wavefront survivors: (distance, window) into the packed
+// best-so-far, as the search kernels would (their cells and z-values are the
+// same, so the distances are bit-identical).
+__global__ void wave_keys_kernel(const float* __restrict__ d, const Cand* __restrict__ cands,
+                                 const int* __restrict__ count, int cap,
+                                 unsigned long long* __restrict__ key) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int n = *count > cap ? 0 : *count;
+    const bool ok = i < n && d[i] == d[i] && d[i] < CDTW_INF;
+    const unsigned long long k =
+        warp_min_key(ok, ok ? d[i] : CDTW_INF, ok ? (uint32_t)cands[i].w : 0xffffffffu);
+    if ((threadIdx.x & 31) == 0 && k != ~0ull) atomicMin(key, k);
 }
 
 // First best-so-far from the seeds' cDTW: the smallest distance, raised by
@@ -429,7 +466,22 @@ int run_search(cdtw_handle h, const float* x, int64_t N, const double* mu, const
             x, mu, sigma, q.zq, q.env, ws.xenv, ws.lbkim, q.M, ws.q1, ws.ctr + 0, ws.key, ws.q2,
             ws.ctr + 1);
     CDTW_LAUNCH(h, "keogh_filter_kernel");
-    // 5. cDTW of the survivors with early abandoning
+    // 5. cDTW of the survivors: as pairwise wavefronts when at most `wcap`
+    //    remain and a window is long enough that a thread per window is
+    //    latency-bound, else with early abandoning
+    const int wcap = (int)std::min<int64_t>(kWaveSurvivors, ws.seed_cap / q.M);
+    const double wcells = (double)q.M * (2.0 * Wp + 1.0) - (double)Wp * (Wp + 1.0);
+    if (Wp <= CDTW_PAIR_MAX_BAND && q.M <= CDTW_MAX_QUERY && wcap >= 32 &&
+        wcells >= kWaveMinCells) {
+        wave_gather_kernel<<<(unsigned)div_up((int64_t)wcap * 32, 256), 256, 0, h->stream>>>(
+            x, mu, sigma, ws.q2, ws.ctr + 1, wcap, q.M, ws.seed_z, ws.ctr + 3);
+        CDTW_LAUNCH(h, "wave_gather_kernel");
+        CDTW_TRY(launch_pair_fwd(h, q.zq, ws.seed_z, wcap, q.M, Wp, euclid, ws.seed_d, nullptr,
+                                 nullptr, nullptr, /*qstride=*/0, ws.ctr + 1, wcap));
+        wave_keys_kernel<<<(unsigned)div_up(wcap, 256), 256, 0, h->stream>>>(
+            ws.seed_d, ws.q2, ws.ctr + 1, wcap, ws.key);
+        CDTW_LAUNCH(h, "wave_keys_kernel");
+    }
     CDTW_TRY(launch_cdtw_search(h, x, N, mu, sigma, ws.q2, ws.ctr + 1, ws.ctr + 3, (int)Nw,
                                 euclid, ws.key));
     if (key_out) *key_out = ws.key;
