@@ -105,7 +105,7 @@ __global__ void wave_keys_kernel(const float* __restrict__ d, const Cand* __rest
 // First best-so-far from the seeds' cDTW: the smallest distance, raised by
 // kSeedBoundSlack relative and 1e-6 per query sample absolute, and paired with
 // no window (index 0xffffffff).  The seed z-values are rounded once from FP64,
-// the search kernels' differ by at most an ulp, so the seed window's own
+// the search kernels' differ by a few ulps at most, so the seed window's own
 // distance as the search kernels compute it lies below this bound (also for
 // an exact match, distance 0): the bound prunes nothing that could be the
 // best, and the best window replaces it in the key.
