@@ -99,8 +99,9 @@ size_t pair_dirs_words(int L, int W);
 int launch_pair_znorm(cdtw_handle h, const float* q, const float* s, int64_t n, int L, float* zq,
                       float* zs, double* hdr);
 // qstride: elements between the queries of consecutive pairs (-1: L; 0: all
-// pairs share the query at zq).  gate: a device count; the launch does
-// nothing when *gate > gate_max (a decision the host cannot see).
+// pairs share the query at zq).  gate: a device count of the pairs present
+// (the first min(n, *gate) run; warps past them exit at once), and the
+// launch does nothing when *gate > gate_max (decisions the host cannot see).
 int launch_pair_fwd(cdtw_handle h, const float* zq, const float* zs, int64_t n, int L, int W,
                     bool euclid, float* D, uint32_t* dirs, uint32_t* rows, uint32_t* cols,
                     int64_t qstride = -1, const int* gate = nullptr, int gate_max = 0);

@@ -44,8 +44,8 @@ struct PairArgs {
     uint32_t* dirs;       // per pair dstride words: 2L-1 rows of G lane elements (path record)
     int dstride;
     int recb, logb;       // shared-record mode: bytes of record and move log per group
-    const int* gate;      // when set and *gate > gate_max the launch does nothing
-    int gate_max;
+    const int* gate;      // when set: a device count of the pairs present (at most n);
+    int gate_max;         // the launch does nothing when it exceeds gate_max
     uint32_t* rows;       // per pair L words: a_i | b_i << 16
     uint32_t* cols;       // per pair L words: c_j | d_j << 16
 };
@@ -377,14 +377,22 @@ template <int C, bool EU, int DM>
 __global__ void __launch_bounds__(kPairThreads, 4) pair_fwd_kernel(const PairArgs a) {
     constexpr bool DIRS = DM != 0;
     extern __shared__ __align__(16) unsigned char smem[];
-    if (a.gate && *a.gate > a.gate_max) return;  // uniform for the whole launch
+    int64_t np = a.n;  // pairs present
+    if (a.gate) {
+        const int c = *a.gate;
+        if (c > a.gate_max) return;  // uniform for the whole launch
+        np = min(np, (int64_t)max(c, 0));
+    }
     const int G = a.G, L = a.L, W = a.W;
     const int tid = threadIdx.x;
     const int l = tid & (G - 1);
     const int gib = tid >> a.lgG;  // group in block
     const int64_t grp = (int64_t)blockIdx.x * (blockDim.x >> a.lgG) + gib;
-    const bool live = grp < a.n;
-    const int64_t pr = live ? grp : a.n - 1;
+    // a warp whose groups all lie past the pairs present has nothing to do
+    // (groups never straddle warps: G is a power of two <= 32)
+    if ((int64_t)blockIdx.x * (blockDim.x >> a.lgG) + ((tid & ~31) >> a.lgG) >= np) return;
+    const bool live = grp < np;
+    const int64_t pr = live ? grp : np - 1;
     const float* sq = a.zq + pr * a.qstride;  // the pair's series (L2-resident; edge lanes read them)
     const float* ss = a.zs + pr * L;
 

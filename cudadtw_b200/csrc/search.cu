@@ -41,7 +41,7 @@ struct SearchWs {
     int* ctr = nullptr;  // [0] n1, [1] n2, [2] work seeds, [3] work main, [4] n seeds
     unsigned long long* key = nullptr;
     float* seed_z = nullptr;  // z-normalised seed windows (seed_cap floats)
-    float* seed_d = nullptr;  // their cDTW (kSeedMax floats)
+    float* seed_d = nullptr;  // their cDTW (max(kSeedMax, kWaveSurvivors) floats)
     int64_t seed_cap = 0;
 };
 
@@ -49,7 +49,7 @@ constexpr int kKimBlock = 256;
 constexpr int kSeedMax = 4096;                     // seed_target's upper limit
 constexpr int64_t kSeedZMax = (int64_t)1 << 24;    // floats of seed windows (64 MB)
 constexpr float kSeedBoundSlack = 1.0f + 1e-4f;
-constexpr int kWaveSurvivors = 512;                // survivors cDTW'd as wavefronts
+constexpr int kWaveSurvivors = 8192;               // survivors cDTW'd as wavefronts (at most)
 constexpr double kWaveMinCells = 4.0e4;            // band cells per window for that
 
 // The seed windows, z-normalised (FP64 arithmetic, rounded once), one row of
@@ -69,10 +69,10 @@ __global__ void seed_gather_kernel(const float* __restrict__ x, const double* __
 
 // The survivors of the bounds when there are at most `cap`, z-normalised
 // exactly as the search kernels do (make_norm / znorm), for their pairwise
-// wavefront cDTW; rows past the survivor count repeat a valid window and are
-// ignored.  Thread 0 starts the search kernels' work counter at cap (they
-// then find nothing left), or at 0 when there are more survivors than cap
-// (the wavefront pass is skipped and they take all).
+// wavefront cDTW (which runs the first *count rows only).  Thread 0 starts
+// the search kernels' work counter at cap (they then find nothing left), or
+// at 0 when there are more survivors than cap (the wavefront pass is skipped
+// and they take all).
 __global__ void wave_gather_kernel(const float* __restrict__ x, const double* __restrict__ mu,
                                    const float* __restrict__ sigma, const Cand* __restrict__ cands,
                                    const int* __restrict__ count, int cap, int M,
@@ -81,8 +81,8 @@ __global__ void wave_gather_kernel(const float* __restrict__ x, const double* __
     const int i = (int)(((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
     const int n = *count;
     if (blockIdx.x == 0 && threadIdx.x == 0) *work = n > cap ? 0 : cap;
-    if (i >= cap || n > cap) return;
-    const int w = i < n ? cands[i].w : (n > 0 ? cands[0].w : 0);
+    if (i >= n || n > cap) return;
+    const int w = cands[i].w;
     const Norm nm = make_norm(mu[w], sigma[w]);
     float* zi = z + (int64_t)i * M;
     for (int j = lane; j < M; j += 32) zi[j] = znorm(nm, __ldg(x + w + j));
@@ -223,9 +223,12 @@ size_t carve_search(int64_t N, int64_t Nw, int M, SearchWs* ws, char* base) {
     ws->envscratch = (float*)take(stream_envelope_scratch_bytes(N));
     ws->ctr = (int*)take(sizeof(int) * 8);
     ws->key = (unsigned long long*)take(sizeof(unsigned long long));
-    ws->seed_cap = std::min<int64_t>(std::min<int64_t>(nblk, kSeedMax) * M, kSeedZMax);
+    // rows of the seed windows (at most kSeedMax) and of the survivors run as
+    // wavefronts (at most kWaveSurvivors)
+    const int64_t rows = std::min<int64_t>(Nw, std::max<int64_t>(kSeedMax, kWaveSurvivors));
+    ws->seed_cap = std::min<int64_t>(rows * M, kSeedZMax);
     ws->seed_z = (float*)take(sizeof(float) * ws->seed_cap);
-    ws->seed_d = (float*)take(sizeof(float) * kSeedMax);
+    ws->seed_d = (float*)take(sizeof(float) * std::max(kSeedMax, kWaveSurvivors));
     return off;
 }
 
