@@ -39,6 +39,10 @@ N_STREAM = 1 << 22
 M_QUERY = 128
 BAND_PCT = (10, 20)
 L2_FLUSH_BYTES = 256 << 20
+# config-1 (M, P) cases timed with UCR_DTW_BIN beside the GPU search (the
+# others take minutes of UCR on every host core)
+UCR_CONFIG1 = {(128, 5), (128, 10), (128, 20), (256, 5), (256, 10), (256, 20), (512, 5),
+               (512, 10), (1024, 5)}
 
 
 def cells(m: int, w: int) -> int:
@@ -312,8 +316,11 @@ def subresults(h, dev) -> dict:
 
     * pruned_search: config 0 (2^20 ECG-like, M=128, W=12) and config 1
       (2^25 metal-like, M in {128,256,512,1024} x P in {5,10,20}): device time
-      of one full search (statistics excluded; they are shared per M),
-      effective GCUPS = windows * cells(M,W) / time, stream samples/s.
+      of one full search (statistics excluded; they are shared per M), stream
+      samples/s, the pruning-inclusive rate windows * cells(M,W) / time, the
+      FP64 oracle's distance at the reported window and the relative error,
+      and, on the same inputs, the location and wall time of the reference's
+      UCR_DTW_BIN on the host cores.
     * batched_search: a 128-query sample of config 2 (2^24 ECG-like stream,
       M ~ U{64..1024}, P in {5,10,20}) as one batched graph call, against the
       same queries as 128 plain searches on the same GPU.
@@ -337,12 +344,15 @@ def subresults(h, dev) -> dict:
         return e0.elapsed_time(e1) / 1e3 / reps, r
 
     # -- pruned search -----------------------------------------------------
+    import oracle
     rows = []
     cases = [("config0 ecg 2^20", synth.ecg_like(1 << 20, seed=0), [(128, 10)], 0.05)]
     cases.append(("config1 metal 2^25", synth.metal_like(1 << 25, seed=1),
                   [(m, p) for m in (128, 256, 512, 1024) for p in (5, 10, 20)], 0.1))
+    ucr_budget_s = 90.0  # wall seconds of UCR_DTW_BIN runs beside the rows
     for name, x, qs, noise in cases:
         dx = torch.from_numpy(x).to(dev)
+        ucr = oracle.UcrShards(x, max_m=1024) if x.size > (1 << 20) else None
         for m, pct in qs:
             q, off = synth.cut_query(x, m, seed=100 + m + pct, noise=noise)
             w = synth.band_from_percent(m, pct)
@@ -351,10 +361,41 @@ def subresults(h, dev) -> dict:
             h.prune_cdtw(dx, avg, std)  # warm
             t, (loc, dist) = dev_time(lambda: h.prune_cdtw(dx, avg, std))
             nwin = x.size - m + 1
-            rows.append({"case": name, "M": m, "P": pct, "W": w, "ms": t * 1e3,
-                         "effective_gcups": nwin * cells(m, w) / t / 1e9,
-                         "samples_per_s": nwin / t, "location": int(loc),
-                         "planted": int(off), "counts": list(h.search_counts())})
+            ref = float(np.sqrt(oracle.cdtw_list(q, x, w, np.array([loc]))[0]))
+            row = {"case": name, "M": m, "P": pct, "W": w, "ms": t * 1e3,
+                   "samples_per_s": nwin / t,
+                   # windows x cells(M, W) / search time: includes what pruning
+                   # skipped, so it is not a hardware cell rate
+                   "pruning_inclusive_gcups": nwin * cells(m, w) / t / 1e9,
+                   "location": int(loc), "planted": int(off),
+                   "counts": list(h.search_counts()),
+                   "fp64_distance": ref, "rel_err": abs(float(dist) - ref) / ref}
+            # the reference's own CPU search on the same inputs (UCR_DTW_BIN
+            # built from its sources): whole stream in one process for the
+            # 2^20 stream, concurrent shard processes (one per host core) on
+            # the 2^25 stream while the time budget lasts
+            if ucr_budget_s > 0 and (ucr is None or (m, pct) in UCR_CONFIG1):
+                if ucr is None:
+                    t0 = time.perf_counter()
+                    uloc, udist, cpu, _ = oracle.ucr_dtw(x, q, oracle.ucr_band_arg(w, m))
+                    wall, cores, cpus = time.perf_counter() - t0, 1, [cpu]
+                else:
+                    uloc, udist, wall, cpus = ucr.search(q, w)
+                    cores = ucr.shards
+                ucr_budget_s -= wall
+                row["ucr_location"] = int(uloc)
+                row["same_location"] = int(uloc) == int(loc)
+                row["ucr_distance"] = udist
+                row["cpu_baseline"] = {"value": nwin / wall, "unit": "samples/s", "cores": cores,
+                                       "kind": "reference",
+                                       "sample": "whole stream; UCR_DTW_BIN wall time" +
+                                       (f" over {cores} concurrent shard processes (M-1 halo)"
+                                        if cores > 1 else ", one process"),
+                                       "ucr_clock_s_total": float(sum(c or 0 for c in cpus))}
+                row["gpu_over_ucr_wall"] = wall / t
+            rows.append(row)
+        if ucr is not None:
+            ucr.__exit__(None, None, None)
         del dx
     out["pruned_search"] = rows
 

@@ -34,6 +34,8 @@ SIGNATURES = {
     "cdtw_prune_cdtw": (c_int, [c_vp, c_vp, c_i64, c_vp, c_vp, c_int, c_i64p, c_f32p]),
     "cdtw_search_host": (c_int, [c_vp, c_vp, c_int, c_vp, c_i64, c_int, c_int, c_i64p, c_f32p]),
     "cdtw_search_counts": (c_int, [c_vp, c_i64p]),
+    "cdtw_search_flag": (c_int, [c_vp, ctypes.POINTER(c_int)]),
+    "cdtw_set_memory_limit": (c_int, [c_vp, ctypes.c_size_t]),
     "cdtw_topk": (c_int, [c_vp, c_vp, c_i64, c_vp, c_vp, c_int, c_int, c_vp, c_vp,
                           ctypes.POINTER(c_int)]),
     "cdtw_set_band_variant": (c_int, [c_vp, c_int, c_int, c_int]),

@@ -210,6 +210,18 @@ class Handle:
                                         _ptr(dists), ctypes.byref(found)))
         return locs[:found.value], dists[:found.value]
 
+    def set_memory_limit(self, nbytes: int) -> None:
+        """Cap the device memory the handle holds (0: no cap); calls that
+        would need more raise CudaDTWError with status CDTW_ENOMEM (2)."""
+        self._check(self._lib.cdtw_set_memory_limit(self._h, int(nbytes)))
+
+    def search_flag(self) -> int:
+        """The reference's termination flag of the last search (the line
+        GPU-DTW prints after "Distance:"): best distance < largest LB_Kim."""
+        f = ctypes.c_int()
+        self._check(self._lib.cdtw_search_flag(self._h, ctypes.byref(f)))
+        return f.value
+
     def search_counts(self):
         """(windows, below bsf after LB_Kim, reaching cDTW) of the last search."""
         c = (ctypes.c_int64 * 3)()
@@ -256,7 +268,7 @@ class Handle:
         return loc.value, dist.value
 
     # -- kernel selection -----------------------------------------------------
-    VARIANTS = {"auto": 0, "register": 1, "strip16": 2, "strip32": 3}
+    VARIANTS = {"auto": 0, "register": 1, "strip16": 2, "strip32": 3, "lane": 4}
 
     def set_band_variant(self, w_lo: int, w_hi: int, variant) -> None:
         """cDTW kernel variant for bands w_lo..w_hi (the autotuner's knob)."""

@@ -63,7 +63,25 @@ def variant_candidates(W: int) -> list[str]:
         out.append("strip16")
     if W >= 31:
         out.append("strip32")
+    if lane_shape(W) is not None:
+        out.append("lane")
     return out
+
+
+def lane_shape(W: int):
+    """(lanes per window group, cells per lane) of the lane-group kernels for
+    band W, or None when they cannot run it: the rule of lane_shape in
+    csrc/cdtw_lane.cu (G in {4, 8, 16, 32}, 18 <= B <= 48, G*B >= 2W+1,
+    (G-1)*B <= 2W, least 3GB + 10G)."""
+    best = None
+    for g in (4, 8, 16, 32):
+        for b in range(18, 49):
+            if g * b < 2 * W + 1 or (g - 1) * b > 2 * W:
+                continue
+            cost = 3 * g * b + 10 * g
+            if best is None or cost < best[0]:
+                best = (cost, g, b)
+    return None if best is None else best[1:]
 
 
 def tune_batched(queries: list, bands: Iterable[int],

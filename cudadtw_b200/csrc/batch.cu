@@ -78,7 +78,7 @@ __device__ void refill_dtw(const BatchQ& Q, const float* __restrict__ x, int n, 
             if (s == S - 1) {
                 atomicMin(Q.key, pack_key(strip_result<R>(Q.sa, ring), (uint32_t)w));
                 active = false;
-            } else if (rmin + (lbk - pre) * kLbSlack >= load_bsf(Q.key)) {
+            } else if (rmin + lb_suffix(lbk, pre, M) * kLbSlack >= load_bsf(Q.key)) {
                 active = false;  // abandoned
             } else {
                 ++s;

@@ -141,7 +141,9 @@ static int build_plan(cdtw_handle h, BatchPlan& p, bool euclid) {
     const size_t o_ctr = take(sizeof(int) * (2 + nl));
     const size_t o_ring =
         take((size_t)blocks * batch_warps_per_block() * ring_stride * sizeof(float));
+    CDTW_TRY(check_memory_limit(h, h->batch_bytes, off, "batched-search plan"));
     CDTW_CUDA(h, cudaMalloc(&p.dmem, off));
+    h->batch_bytes = off;
     CDTW_CUDA(h, cudaMallocHost(&p.hpin, raw_floats * sizeof(float) + nq * 8 + 64));
     p.raw_floats = raw_floats;
     char* d = (char*)p.dmem;
@@ -306,6 +308,7 @@ extern "C" int cdtw_search_batched(cdtw_handle h, const float* d_subject, int64_
     if (!same) {
         CDTW_CUDA(h, cudaStreamSynchronize(h->own_stream));
         p.release();
+        h->batch_bytes = 0;
         p.subject = d_subject;
         p.N = N;
         p.metric = metric;
@@ -317,6 +320,7 @@ extern "C" int cdtw_search_batched(cdtw_handle h, const float* d_subject, int64_
         const int st = build_plan(h, p, metric == CDTW_EUCLIDEAN);
         if (st != CDTW_OK) {
             p.release();
+            h->batch_bytes = 0;
             return st;
         }
     }
@@ -353,6 +357,7 @@ void batch_plan_release(cdtw_handle h) {
         p->release();
         delete p;
         h->batch = nullptr;
+        h->batch_bytes = 0;
     }
 }
 }  // namespace cdtw

@@ -42,9 +42,13 @@ __global__ void __launch_bounds__(256)
 lb_kim_kernel(const float* __restrict__ x, const double* __restrict__ mu,
               const float* __restrict__ sigma, const float* __restrict__ zq, int M, int Nw,
               const int32_t* __restrict__ idx, int L, float* __restrict__ out,
-              unsigned long long* __restrict__ seeds) {
+              unsigned long long* __restrict__ seeds, unsigned* __restrict__ bmax) {
     __shared__ unsigned long long best;
-    if (seeds && threadIdx.x == 0) best = ~0ull;
+    __shared__ unsigned vmax;
+    if (seeds && threadIdx.x == 0) {
+        best = ~0ull;
+        vmax = 0u;
+    }
     if (seeds) __syncthreads();
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     float v = CDTW_INF;
@@ -60,11 +64,19 @@ lb_kim_kernel(const float* __restrict__ x, const double* __restrict__ mu,
         out[t] = v;
     }
     if (seeds) {  // the block's smallest bound: a seed window for the search
-        const unsigned long long k =
-            warp_min_key(t < L && w >= 0 && w < Nw && v == v, v, (uint32_t)w);
-        if ((threadIdx.x & 31) == 0 && k != ~0ull) atomicMin(&best, k);  // one per warp
+        const bool ok = t < L && w >= 0 && w < Nw && v == v;
+        const unsigned long long k = warp_min_key(ok, v, (uint32_t)w);
+        // and its largest (bounds are >= 0: their bits order as unsigned)
+        const unsigned mx = __reduce_max_sync(0xffffffffu, ok ? __float_as_uint(v) : 0u);
+        if ((threadIdx.x & 31) == 0) {  // one shared atomic of each kind per warp
+            if (k != ~0ull) atomicMin(&best, k);
+            atomicMax(&vmax, mx);
+        }
         __syncthreads();
-        if (threadIdx.x == 0) seeds[blockIdx.x] = best;
+        if (threadIdx.x == 0) {
+            seeds[blockIdx.x] = best;
+            bmax[blockIdx.x] = vmax;
+        }
     }
 }
 
@@ -82,8 +94,10 @@ constexpr int kEnvSmemFloats = 50176;  // 196 KB
 // fit); otherwise one buffer updated in place in increasing chunks.
 template <bool PING>
 __global__ void __launch_bounds__(kEnvThreads)
-env_window_kernel(const float* __restrict__ x, int64_t N, int W, int T, float2* __restrict__ env) {
+env_window_kernel(const float* __restrict__ x, int64_t N, int W, int T, float2* __restrict__ env,
+                  const int* __restrict__ gate, int gate_max) {
     extern __shared__ float esm[];
+    if (gate && *(const volatile int*)gate <= gate_max) return;  // not needed by this search
     const int K = 2 * W + 1;
     const int S = T + 2 * W;
     float* lo = esm;
@@ -180,7 +194,7 @@ lb_keogh_kernel(const float* __restrict__ x, const double* __restrict__ mu,
 
 int launch_lb_kim(cdtw_handle h, const float* x, int64_t N, const double* mu, const float* sigma,
                   const int32_t* idx, int64_t L, bool euclid, float* out,
-                  unsigned long long* seeds) {
+                  unsigned long long* seeds, unsigned* bmax) {
     const QueryPack& q = h->q;
     if (q.M < 11)
         return set_error(h, CDTW_EINVAL,
@@ -190,10 +204,10 @@ int launch_lb_kim(cdtw_handle h, const float* x, int64_t N, const double* mu, co
     const unsigned blocks = (unsigned)div_up(L, 256);
     if (euclid)
         lb_kim_kernel<true><<<blocks, 256, 0, h->stream>>>(x, mu, sigma, q.zq, q.M, Nw, idx,
-                                                            (int)L, out, seeds);
+                                                            (int)L, out, seeds, bmax);
     else
         lb_kim_kernel<false><<<blocks, 256, 0, h->stream>>>(x, mu, sigma, q.zq, q.M, Nw, idx,
-                                                             (int)L, out, seeds);
+                                                             (int)L, out, seeds, bmax);
     CDTW_LAUNCH(h, "lb_kim_kernel");
     return CDTW_OK;
 }
@@ -201,7 +215,7 @@ int launch_lb_kim(cdtw_handle h, const float* x, int64_t N, const double* mu, co
 size_t stream_envelope_scratch_bytes(int64_t) { return 0; }
 
 int launch_stream_envelope(cdtw_handle h, const float* x, int64_t N, int W, float*,
-                           float2* env) {
+                           float2* env, const int* gate, int gate_max) {
     // tile: at least 2048 outputs (or 2W when the halo is larger); four
     // arrays (ping-pong) when they fit the shared-memory budget, else two
     if (kEnvSmemFloats / 2 - 2 * W < 1)
@@ -213,11 +227,11 @@ int launch_stream_envelope(cdtw_handle h, const float* x, int64_t N, int W, floa
     const void* k = ping ? (const void*)env_window_kernel<true> : (const void*)env_window_kernel<false>;
     CDTW_CUDA(h, cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     if (ping)
-        env_window_kernel<true><<<(unsigned)div_up(N, T), kEnvThreads, smem, h->stream>>>(x, N, W, T,
-                                                                                     env);
+        env_window_kernel<true><<<(unsigned)div_up(N, T), kEnvThreads, smem, h->stream>>>(
+            x, N, W, T, env, gate, gate_max);
     else
-        env_window_kernel<false><<<(unsigned)div_up(N, T), kEnvThreads, smem, h->stream>>>(x, N, W,
-                                                                                      T, env);
+        env_window_kernel<false><<<(unsigned)div_up(N, T), kEnvThreads, smem, h->stream>>>(
+            x, N, W, T, env, gate, gate_max);
     CDTW_LAUNCH(h, "env_window_kernel");
     return CDTW_OK;
 }

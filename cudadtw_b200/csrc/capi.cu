@@ -25,8 +25,20 @@ int check_cuda(cdtw_handle h, cudaError_t e, const char* what) {
     return set_error(h, CDTW_ECUDA, "%s: %s", what, cudaGetErrorString(e));
 }
 
+int check_memory_limit(cdtw_handle h, size_t freed, size_t bytes, const char* what) {
+    if (h->mem_limit == 0) return CDTW_OK;
+    const size_t held = h->ws_bytes + h->qmem_bytes + h->ring_bytes + h->batch_bytes;
+    if (held - std::min(held, freed) + bytes <= h->mem_limit) return CDTW_OK;
+    return set_error(h, CDTW_ENOMEM,
+                     "%s needs %zu bytes of device memory: above the handle's limit of %zu "
+                     "(holding %zu)",
+                     what, bytes, h->mem_limit, held);
+}
+
 int ensure_workspace(cdtw_handle h, size_t bytes) {
     if (bytes <= h->ws_bytes) return CDTW_OK;
+    CDTW_TRY(check_memory_limit(h, h->ws_bytes, round_up((int64_t)bytes, 1 << 20),
+                                "work area"));
     if (h->ws) {
         // the old block may still be in use by queued work on the stream
         CDTW_CUDA(h, cudaStreamSynchronize(h->stream));
@@ -53,7 +65,7 @@ struct Carver {
 
 static int ensure_query_mem(cdtw_handle h, int M, int W) {
     QueryPack& q = h->q;
-    const int lq = (int)round_up(M + 2 * W + 8, 4);
+    const int lq = qpad_len(M, W);
     Carver c;
     const size_t o_qpad = c.take<float>(4 * (size_t)lq);
     const size_t o_env = c.take<float2>(M);
@@ -63,6 +75,7 @@ static int ensure_query_mem(cdtw_handle h, int M, int W) {
     const size_t o_qrev = c.take<float>(4 * (size_t)lqr);
     const size_t bytes = c.off;
     if (bytes > h->qmem_bytes) {
+        CDTW_TRY(check_memory_limit(h, h->qmem_bytes, bytes, "query pack"));
         if (h->qmem) {
             CDTW_CUDA(h, cudaStreamSynchronize(h->stream));
             CDTW_CUDA(h, cudaFree(h->qmem));
@@ -94,17 +107,23 @@ static int finish_search(cdtw_handle h, const unsigned long long* key, const int
     char* pin = (char*)h->pinned;
     CDTW_CUDA(h, cudaMemcpyAsync(pin, key, sizeof(unsigned long long), cudaMemcpyDeviceToHost,
                                  h->stream));
-    CDTW_CUDA(h, cudaMemcpyAsync(pin + 8, ctr, sizeof(int) * 2, cudaMemcpyDeviceToHost,
+    CDTW_CUDA(h, cudaMemcpyAsync(pin + 8, ctr, sizeof(int) * 6, cudaMemcpyDeviceToHost,
                                  h->stream));
     CDTW_CUDA(h, cudaStreamSynchronize(h->stream));
     unsigned long long k;
-    int c[2];
+    int c[6];
     memcpy(&k, pin, 8);
-    memcpy(c, pin + 8, 8);
+    memcpy(c, pin + 8, sizeof(c));
     h->last_counts[0] = Nw;
     h->last_counts[1] = c[0];
     h->last_counts[2] = c[1];
-    if (k == ~0ull) return set_error(h, CDTW_ECUDA, "search produced no result");
+    // the reference's termination flag: best < largest LB_Kim (ctr[5] holds
+    // its bits; both are >= 0)
+    h->last_flag = (uint32_t)(k >> 32) < (uint32_t)c[5] ? 1 : 0;
+    if (k == ~0ull)
+        return set_error(h, CDTW_EINVAL,
+                         "no window has a finite distance (NaN or Inf in the query or in every "
+                         "window of the subject)");
     if ((uint32_t)k == 0xffffffffu)  // only the seeds' upper bound: no window beat it
         return set_error(h, CDTW_ECUDA, "search kept the seed bound, not a window");
     const uint32_t bits = (uint32_t)(k >> 32);
@@ -285,7 +304,8 @@ int cdtw_all_windows_host(cdtw_handle h, const float* h_query, int M, const floa
     const bool eu = metric == CDTW_EUCLIDEAN;
     cudaStream_t const user = h->stream;
     // strip kernels share the handle's ring buffer: their chunks stay on one stream
-    const bool alternate = choose_variant(h, h->q.W) == CDTW_VARIANT_REGISTER;
+    const int variant = choose_variant(h, h->q.W);
+    const bool alternate = variant == CDTW_VARIANT_REGISTER || variant == CDTW_VARIANT_LANE;
     cudaStream_t const comp[2] = {user, alternate ? h->xfer[2] : user};
     int64_t copied = 0;  // samples already on the device
     for (int i = 0; i < nch; ++i) {
@@ -328,7 +348,7 @@ int cdtw_lb_kim(cdtw_handle h, const float* d_subject, int64_t N, const double* 
     if (L < 0 || L > INT32_MAX) return set_error(h, CDTW_EINVAL, "bad index count");
     CDTW_CUDA(h, cudaSetDevice(h->device));
     return launch_lb_kim(h, d_subject, N, d_avg, d_std, d_indices, L, metric == CDTW_EUCLIDEAN,
-                         d_out, nullptr);
+                         d_out);
 }
 
 int cdtw_lb_keogh(cdtw_handle h, const float* d_subject, int64_t N, const double* d_avg,
@@ -370,7 +390,7 @@ int cdtw_prune_cdtw(cdtw_handle h, const float* d_subject, int64_t N, const doub
     if (N < M) return set_error(h, CDTW_EINVAL, "subject shorter than query");
     if (N - M + 1 > INT32_MAX) return set_error(h, CDTW_EUNSUPPORTED, "too many windows");
     CDTW_CUDA(h, cudaSetDevice(h->device));
-    CDTW_TRY(ensure_workspace(h, search_workspace_bytes(N, M)));
+    CDTW_TRY(ensure_workspace(h, search_workspace_bytes(N, M, h->q.W)));
     unsigned long long* key;
     int* ctr;
     CDTW_TRY(run_search(h, d_subject, N, d_avg, d_std, metric == CDTW_EUCLIDEAN, (char*)h->ws,
@@ -392,7 +412,7 @@ int cdtw_topk(cdtw_handle h, const float* d_subject, int64_t N, const double* d_
     if (M < 11) return set_error(h, CDTW_EUNSUPPORTED, "top-k search needs M >= 11");
     if (!valid_metric(metric)) return set_error(h, CDTW_EINVAL, "bad metric %d", metric);
     CDTW_CUDA(h, cudaSetDevice(h->device));
-    CDTW_TRY(ensure_workspace(h, topk_workspace_bytes(N, M)));
+    CDTW_TRY(ensure_workspace(h, topk_workspace_bytes(N, M, h->q.W)));
     std::vector<unsigned long long> picks;
     CDTW_TRY(run_topk(h, d_subject, N, d_avg, d_std, metric == CDTW_EUCLIDEAN, k,
                       (char*)h->ws, &picks));
@@ -421,7 +441,7 @@ int cdtw_search_host(cdtw_handle h, const float* h_query, int M, const float* h_
     const size_t o_x = c.take<float>(N);
     const size_t o_mu = c.take<double>(Nw);
     const size_t o_sd = c.take<float>(Nw);
-    const size_t o_ws = c.take<char>(search_workspace_bytes(N, M));
+    const size_t o_ws = c.take<char>(search_workspace_bytes(N, M, std::min(W, M - 1)));
     CDTW_TRY(ensure_workspace(h, c.off));
     char* base = (char*)h->ws;
     float* dx = (float*)(base + o_x);
@@ -642,9 +662,21 @@ int cdtw_pair_bwd(cdtw_handle h, const float* d_q, const float* d_s, int64_t n, 
 
 int cdtw_set_band_variant(cdtw_handle h, int w_lo, int w_hi, int variant) {
     if (!h) return CDTW_EINVAL;
-    if (variant < CDTW_VARIANT_AUTO || variant > CDTW_VARIANT_STRIP32 || w_lo < 0 || w_hi < w_lo)
+    if (variant < CDTW_VARIANT_AUTO || variant > CDTW_VARIANT_LANE || w_lo < 0 || w_hi < w_lo)
         return set_error(h, CDTW_EINVAL, "bad band range or variant");
     for (int w = w_lo; w <= w_hi && w < CDTW_MAX_QUERY; ++w) h->band_variant[w] = (unsigned char)variant;
+    return CDTW_OK;
+}
+
+int cdtw_set_memory_limit(cdtw_handle h, size_t bytes) {
+    if (!h) return CDTW_EINVAL;
+    h->mem_limit = bytes;
+    return CDTW_OK;
+}
+
+int cdtw_search_flag(cdtw_handle h, int* flag) {
+    if (!h || !flag) return CDTW_EINVAL;
+    *flag = h->last_flag;
     return CDTW_OK;
 }
 

@@ -1,0 +1,11 @@
+// Lane-block cDTW kernels for B = 18..25 cells per lane (one of four
+// translation units of the instantiation range, compiled in parallel).
+#include "cdtw_lane.cuh"
+
+namespace cdtw {
+
+void lane_fill_part0(LaneKernel* eu, LaneKernel* mh, LaneKernel* seu, LaneKernel* smh) {
+    LaneRange<18, 25>::fill(eu, mh, seu, smh);
+}
+
+}  // namespace cdtw

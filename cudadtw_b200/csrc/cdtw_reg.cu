@@ -56,10 +56,15 @@ int max_register_band() { return kMaxRegW; }
 
 int choose_variant(cdtw_handle h, int W) {
     int v = (W >= 0 && W < CDTW_MAX_QUERY) ? h->band_variant[W] : 0;
+    int G, B;
+    const bool lane = lane_shape(W, &G, &B) && h->q.lq >= lane_qpad_min(h->q.M, W);
     if (v == CDTW_VARIANT_REGISTER && W > kMaxRegW) v = 0;
     if (v == CDTW_VARIANT_STRIP16 && W < 15) v = 0;
     if (v == CDTW_VARIANT_STRIP32 && W < 31) v = 0;
-    if (v == 0) v = (W <= kMaxRegW) ? CDTW_VARIANT_REGISTER : CDTW_VARIANT_STRIP16;
+    if (v == CDTW_VARIANT_LANE && !lane) v = 0;
+    if (v == 0)
+        v = (W <= kMaxRegW) ? CDTW_VARIANT_REGISTER
+                            : (lane ? CDTW_VARIANT_LANE : CDTW_VARIANT_STRIP16);
     return v;
 }
 
@@ -73,6 +78,9 @@ int launch_cdtw_search(cdtw_handle h, const float* x, int64_t N, const double* m
     const QueryPack& q = h->q;
     if (max_count <= 0) return CDTW_OK;
     const int variant = choose_variant(h, q.W);
+    if (variant == CDTW_VARIANT_LANE)
+        return launch_cdtw_lane_search(h, x, N, mu, sigma, cands, count, work, max_count, euclid,
+                                       key);
     if (variant != CDTW_VARIANT_REGISTER)
         return launch_cdtw_strip_search(h, x, N, mu, sigma, cands, count, work, max_count,
                                         euclid, variant == CDTW_VARIANT_STRIP16 ? 16 : 32, key);
@@ -99,6 +107,8 @@ int launch_cdtw_windows(cdtw_handle h, const float* x, int64_t N, const double* 
     const QueryPack& q = h->q;
     const int Nw = (int)(N - q.M + 1);
     const int variant = q.qrev ? choose_variant(h, q.W) : CDTW_VARIANT_REGISTER;
+    if (variant == CDTW_VARIANT_LANE)
+        return launch_cdtw_lane(h, x, N, mu, sigma, idx, L, euclid, out);
     if (variant != CDTW_VARIANT_REGISTER || q.W > kMaxRegW) {
         if (!q.qrev)
             return set_error(h, CDTW_EUNSUPPORTED, "band W=%d above the register-band limit %d",

@@ -240,7 +240,8 @@ __device__ __forceinline__ float reg_window_dtw(const float4* sq4, int lq4,
             float rmin = prev[0];
 #pragma unroll
             for (int k = 1; k < B; k += 2) rmin = min3f(rmin, prev[k], prev[k + 1]);
-            alive = alive && (rmin + (lbk - pre) * kLbSlack < (kAhead ? bsf_early : load_bsf(key)));
+            alive = alive && (rmin + lb_suffix(lbk, pre, M) * kLbSlack <
+                              (kAhead ? bsf_early : load_bsf(key)));
             if (!__any_sync(0xffffffffu, alive)) return CDTW_INF;
         }
     }

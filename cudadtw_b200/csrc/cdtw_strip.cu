@@ -85,6 +85,7 @@ int prepare_strip(cdtw_handle h, K k, const float* x, int64_t N, const double* m
         1, std::min<int64_t>(want, (int64_t)std::max(per_sm, 1) * h->sm_count));
     const size_t ring_bytes = (size_t)(*blocks) * kStripWarps * a->P * 32 * sizeof(float);
     if (ring_bytes > h->ring_bytes) {
+        CDTW_TRY(check_memory_limit(h, h->ring_bytes, ring_bytes, "strip rings"));
         if (h->ring) {
             CDTW_CUDA(h, cudaStreamSynchronize(h->stream));
             CDTW_CUDA(h, cudaFree(h->ring));

@@ -262,7 +262,7 @@ __device__ __forceinline__ float strip_dtw(const StripArgs& a, int w, float* rin
         strip_pass<R, EU, SEARCH>(a, xw, nm, s * R, ring, qenv, pre, rmin);
         if (SEARCH && s * R + R < a.M) {  // the strip's last row is a real row before M-1
             const float bsf = load_bsf(key);
-            alive = alive && (rmin + (lbk - pre) * kLbSlack < bsf);
+            alive = alive && (rmin + lb_suffix(lbk, pre, a.M) * kLbSlack < bsf);
             if (!__any_sync(0xffffffffu, alive)) return CDTW_INF;
         }
     }

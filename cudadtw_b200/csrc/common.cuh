@@ -71,10 +71,15 @@ struct cdtw_handle_s {
     size_t qmem_bytes = 0;
     cdtw::QueryPack q;
     bool has_query = false;
+    // cap on the device memory the handle holds (0: none), cdtw_set_memory_limit
+    size_t mem_limit = 0;
+    size_t batch_bytes = 0;  // device memory of the cached batched-search plan
     // small pinned host buffer for scalar results
     void* pinned = nullptr;
     // stage counts of the last search: windows, after LB_Kim, after LB_Keogh
     int64_t last_counts[4] = {0, 0, 0, 0};
+    // the last search's best distance lies below the largest LB_Kim
+    int last_flag = 0;
     // cDTW kernel variant per band (0 = built-in rule); set by the autotuner
     unsigned char band_variant[CDTW_MAX_QUERY] = {0};
     // host-buffer pipeline (cdtw_all_windows_host): copy-in, copy-out and a
@@ -90,7 +95,7 @@ namespace cdtw {
 int set_error(cdtw_handle h, int status, const char* fmt, ...);
 void batch_plan_release(cdtw_handle h);
 // top-k non-overlapping matches (search.cu)
-size_t topk_workspace_bytes(int64_t N, int M);
+size_t topk_workspace_bytes(int64_t N, int M, int W);
 int run_topk(cdtw_handle h, const float* x, int64_t N, const double* mu, const float* sigma,
              bool euclid, int k, char* ws_base, std::vector<unsigned long long>* picks);
 // pairwise cDTW forward / backward (pair.cu)
@@ -110,6 +115,9 @@ int launch_pair_bwd(cdtw_handle h, const float* q, const float* s, int64_t n, in
                     const float* dD, bool euclid, float* dq, float* ds);
 int check_cuda(cdtw_handle h, cudaError_t e, const char* what);
 int ensure_workspace(cdtw_handle h, size_t bytes);
+// CDTW_ENOMEM when the handle would hold more than its memory limit after
+// releasing `freed` bytes and allocating `bytes` more.
+int check_memory_limit(cdtw_handle h, size_t freed, size_t bytes, const char* what);
 
 #define CDTW_TRY(expr)                        \
     do {                                      \
@@ -246,6 +254,17 @@ __host__ __device__ inline int seed_target(int M, int W) {
 // is below the best (a bound prunes only if it exceeds bsf by 1e-4).
 constexpr float kLbSlack = 1.0f - 1e-4f;
 
+// The forward LB_Keogh of the rows after a prefix, as a certain lower bound:
+// lbk (all M rows) and pre (the prefix) are FP32 sums of non-negative terms,
+// each within (M-1) * 2^-24 relative of its exact value whatever the order of
+// summation (the filter kernels and the cDTW kernels sum in different orders
+// and with or without fused multiply-adds), so lbk (1 - e) - pre (1 + e) with
+// e = M * 1.2e-7 never exceeds the exact remainder.
+__device__ __forceinline__ float lb_suffix(float lbk, float pre, int M) {
+    const float e = (float)M * 1.2e-7f;
+    return fmaxf(fmaf(lbk, 1.f - e, -pre * (1.f + e)), 0.f);
+}
+
 __device__ __forceinline__ float key_dist(unsigned long long k) {
     return __uint_as_float((unsigned)(k >> 32));
 }
@@ -285,17 +304,30 @@ int launch_cdtw_strip(cdtw_handle h, const float* x, int64_t N, const double* mu
                       const float* sigma, const int32_t* idx, int64_t L, bool euclid, int R,
                       float* out);
 int strip_rows_default(int W);
+// Lane-block kernels (cdtw_lane.cu): band spread over G lanes of B cells.
+bool lane_shape(int W, int* G, int* B);
+int lane_qpad_min(int M, int W);  // floats per query copy they read
+int launch_cdtw_lane(cdtw_handle h, const float* x, int64_t N, const double* mu,
+                     const float* sigma, const int32_t* idx, int64_t L, bool euclid, float* out);
+int launch_cdtw_lane_search(cdtw_handle h, const float* x, int64_t N, const double* mu,
+                            const float* sigma, const Cand* cands, const int* count, int* work,
+                            int max_count, bool euclid, unsigned long long* key);
+// floats per shifted query copy (QueryPack::lq) of a handle's query pack
+inline int qpad_len(int M, int W) { return (int)(((int64_t)M + 2 * W + 56 + 3) / 4 * 4); }
 // Kernel choice for band W: CDTW_VARIANT_REGISTER (one thread per window, band
 // in registers, W <= 96), CDTW_VARIANT_STRIP16 / STRIP32 (strips of 16 / 32
-// rows, W >= 15 / 31).
+// rows, W >= 15 / 31), CDTW_VARIANT_LANE (band over a lane group, 27 <= W <=
+// 767).
 int choose_variant(cdtw_handle h, int W);
 int max_register_band();
 int launch_lb_kim(cdtw_handle h, const float* x, int64_t N, const double* mu, const float* sigma,
                   const int32_t* idx, int64_t L, bool euclid, float* out,
-                  unsigned long long* seeds);
+                  unsigned long long* seeds = nullptr, unsigned* bmax = nullptr);
 size_t stream_envelope_scratch_bytes(int64_t N);
+// gate: when set, the kernel does nothing if *gate <= gate_max (a device
+// count the host cannot see, e.g. the LB_Kim survivors of a search).
 int launch_stream_envelope(cdtw_handle h, const float* x, int64_t N, int W, float* scratch,
-                           float2* env);
+                           float2* env, const int* gate = nullptr, int gate_max = 0);
 int launch_lb_keogh(cdtw_handle h, const float* x, int64_t N, const double* mu,
                     const float* sigma, const float2* xenv, const int32_t* idx, int64_t L,
                     bool euclid, float* fwd, float* rev);
@@ -304,7 +336,7 @@ int launch_lb_keogh(cdtw_handle h, const float* x, int64_t N, const double* mu,
 int launch_cdtw_search(cdtw_handle h, const float* x, int64_t N, const double* mu,
                        const float* sigma, const Cand* cands, const int* count, int* work,
                        int max_count, bool euclid, unsigned long long* key);
-size_t search_workspace_bytes(int64_t N, int M);
+size_t search_workspace_bytes(int64_t N, int M, int W);
 int run_search(cdtw_handle h, const float* x, int64_t N, const double* mu, const float* sigma,
                bool euclid, char* ws_base, unsigned long long** key_out, int** ctr_out);
 

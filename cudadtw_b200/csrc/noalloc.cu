@@ -16,8 +16,14 @@
 // library holds it (CDTW_NOALLOC_SCRATCH_BYTES, about 12.3 MiB) until the
 // process exits.  Host code cannot use the array's name as a device address;
 // the first call on each device looks the address up with
-// cudaGetSymbolAddress while that device is current and keeps it.
+// cudaGetSymbolAddress while that device is current and keeps it, together
+// with the unique ID of the CUDA context it belongs to.  A later call in a
+// different context (after cudaDeviceReset, or a released and re-created
+// primary context, where the module loads again and the array may move)
+// looks the address up again.
 #include "common.cuh"
+
+#include <cuda.h>  // CUcontext / CUresult types only; the driver calls are resolved at run time
 
 #include <mutex>
 
@@ -43,15 +49,56 @@ static __device__ __align__(256) unsigned char noalloc_scratch[CDTW_NOALLOC_SCRA
 constexpr int kMaxDevices = 128;
 std::mutex g_setup_mu;
 unsigned char* g_scratch_addr[kMaxDevices] = {nullptr};
+unsigned long long g_scratch_ctx[kMaxDevices] = {0};  // context ID the address belongs to
 
-// Device address of the array on the current device (looked up once per device).
+// Driver entry points for the current context's unique ID, resolved through
+// the runtime (the library does not link libcuda itself).
+using CtxGetCurrentFn = CUresult (*)(CUcontext*);
+using CtxGetIdFn = CUresult (*)(CUcontext, unsigned long long*);
+CtxGetCurrentFn g_ctx_current = nullptr;
+CtxGetIdFn g_ctx_id = nullptr;
+bool g_ctx_fns_tried = false;
+
+// Unique ID of the calling thread's current context; 0 when there is none yet
+// (the runtime creates the primary context on its first real call) or the
+// driver cannot tell.
+unsigned long long current_context_id() {
+    if (!g_ctx_fns_tried) {
+        g_ctx_fns_tried = true;
+        void* f1 = nullptr;
+        void* f2 = nullptr;
+        cudaDriverEntryPointQueryResult r1, r2;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f1, cudaEnableDefault, &r1) ==
+                cudaSuccess &&
+            r1 == cudaDriverEntryPointSuccess &&
+            cudaGetDriverEntryPoint("cuCtxGetId", &f2, cudaEnableDefault, &r2) == cudaSuccess &&
+            r2 == cudaDriverEntryPointSuccess) {
+            g_ctx_current = (CtxGetCurrentFn)f1;
+            g_ctx_id = (CtxGetIdFn)f2;
+        }
+        cudaGetLastError();
+    }
+    if (!g_ctx_current || !g_ctx_id) return 0;
+    CUcontext ctx = nullptr;
+    unsigned long long id = 0;
+    if (g_ctx_current(&ctx) != CUDA_SUCCESS || !ctx) return 0;
+    if (g_ctx_id(ctx, &id) != CUDA_SUCCESS) return 0;
+    return id;
+}
+
+// Device address of the array on the current device: looked up once per
+// device and context (cudaGetSymbolAddress with the device current), reused
+// while the context stays the same.
 cudaError_t scratch_address(int dev, unsigned char** out) {
     std::lock_guard<std::mutex> lock(g_setup_mu);
-    if (!g_scratch_addr[dev]) {
+    const unsigned long long ctx = current_context_id();
+    if (!g_scratch_addr[dev] || ctx == 0 || ctx != g_scratch_ctx[dev]) {
         void* p = nullptr;
         const cudaError_t e = cudaGetSymbolAddress(&p, noalloc_scratch);
         if (e != cudaSuccess) return e;
         g_scratch_addr[dev] = (unsigned char*)p;
+        // the lookup made the context current if there was none before
+        g_scratch_ctx[dev] = ctx != 0 ? ctx : current_context_id();
     }
     *out = g_scratch_addr[dev];
     return cudaSuccess;

@@ -184,6 +184,7 @@ extern "C" int cdtw_refine_templates(cdtw_handle h, const float* d_subject, int6
     const size_t o_loss = c.take<float>((size_t)(steps + 1) * nt);
     CDTW_CUDA(h, cudaSetDevice(h->device));
     char* base = nullptr;
+    CDTW_TRY(check_memory_limit(h, 0, c.off, "template refinement"));
     CDTW_CUDA(h, cudaMalloc(&base, c.off));
     struct Cleanup {
         char* p;

@@ -13,12 +13,15 @@
 //   2. cDTW of the seed windows -> first best-so-far, a packed
 //      (distance, window) key updated by atomicMin.
 //   3. Compaction of the windows whose LB_Kim is below the best-so-far.
-//   4. Forward LB_Keogh (query envelope) and reverse LB_Keogh (stream
-//      envelope, as UCR_DTW_BIN.cpp:262-282) of those, with a warp-level exit
-//      once every lane's bound passed the best-so-far; survivors keep their
-//      best bound and their forward LB_Keogh.
+//   4. Forward LB_Keogh (query envelope) and reverse LB_Keogh (data
+//      envelope, as UCR_DTW_BIN.cpp:262-282) of those, abandoned once the
+//      bound passed the best-so-far; survivors keep their best bound and
+//      their forward LB_Keogh.  Few, scattered survivors: a warp per window
+//      with the window's own envelope; many: the envelope of the whole stream
+//      and a thread per window (the count is read on the device).
 //   5. cDTW of the survivors with early abandoning against the live
-//      best-so-far, folded into the key.
+//      best-so-far, folded into the key: as pairwise wavefronts when few and
+//      long, else by the register-band (W <= 96) or lane-group kernels.
 // No sort, no host loop; graph-capturable launch sequence.
 #include "common.cuh"
 
@@ -33,12 +36,14 @@ namespace {
 struct SearchWs {
     float* lbkim = nullptr;
     unsigned long long* seeds = nullptr;
+    unsigned* bmax = nullptr;  // largest LB_Kim of each block (float bits)
     Cand* seed_cands = nullptr;
     int* q1 = nullptr;
     Cand* q2 = nullptr;
     float2* xenv = nullptr;
     float* envscratch = nullptr;
-    int* ctr = nullptr;  // [0] n1, [1] n2, [2] work seeds, [3] work main, [4] n seeds
+    // [0] n1, [1] n2, [2] work seeds, [3] work main, [4] n seeds, [5] largest LB_Kim (bits)
+    int* ctr = nullptr;
     unsigned long long* key = nullptr;
     float* seed_z = nullptr;  // z-normalised seed windows (seed_cap floats)
     float* seed_d = nullptr;  // their cDTW (max(kSeedMax, kWaveSurvivors) floats)
@@ -118,15 +123,24 @@ __global__ void seed_bound_kernel(const float* __restrict__ d, const Cand* __res
     if ((threadIdx.x & 31) == 0 && k != ~0ull) atomicMin(key, k);
 }
 
-// Seed candidates: the smallest LB_Kim window of each group of G blocks.
-__global__ void seeds_to_cands_kernel(const unsigned long long* __restrict__ seeds, int nblk,
-                                      int G, Cand* __restrict__ cands, int* __restrict__ nseeds) {
+// Seed candidates: the smallest LB_Kim window of each group of G blocks; the
+// largest LB_Kim of all windows into *kmax (float bits).
+__global__ void seeds_to_cands_kernel(const unsigned long long* __restrict__ seeds,
+                                      const unsigned* __restrict__ bmax, int nblk, int G,
+                                      Cand* __restrict__ cands, int* __restrict__ nseeds,
+                                      unsigned* __restrict__ kmax) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int n = (nblk + G - 1) / G;
     if (i == 0) *nseeds = n;
-    if (i >= n) return;
     unsigned long long k = ~0ull;
-    for (int b = i * G; b < min(nblk, (i + 1) * G); ++b) k = min(k, seeds[b]);
+    unsigned mx = 0u;
+    for (int b = i * G; b < min(nblk, (i + 1) * G); ++b) {
+        k = min(k, seeds[b]);
+        mx = max(mx, bmax[b]);
+    }
+    mx = __reduce_max_sync(0xffffffffu, mx);
+    if ((threadIdx.x & 31) == 0 && mx) atomicMax(kmax, mx);
+    if (i >= n) return;
     Cand c;
     c.w = (k == ~0ull) ? 0 : (int)(uint32_t)k;
     c.lb = (k == ~0ull) ? CDTW_INF : 0.f;  // empty block: never started
@@ -161,8 +175,9 @@ keogh_filter_kernel(const float* __restrict__ x, const double* __restrict__ mu,
                     const float2* __restrict__ qenv, const float2* __restrict__ xenv,
                     const float* __restrict__ lbkim, int M, const int* __restrict__ q1,
                     const int* __restrict__ n1p, const unsigned long long* key,
-                    Cand* __restrict__ q2, int* __restrict__ n2) {
+                    Cand* __restrict__ q2, int* __restrict__ n2, int sparse_max) {
     const int n1 = *(const volatile int*)n1p;
+    if (n1 <= sparse_max) return;  // keogh_sparse_kernel takes few survivors
     const float bsf = load_bsf(key);
     const float lim = bsf / kLbSlack;  // bound value at which a window is pruned
     const int lane = threadIdx.x & 31;
@@ -206,7 +221,178 @@ keogh_filter_kernel(const float* __restrict__ x, const double* __restrict__ mu,
     }
 }
 
-size_t carve_search(int64_t N, int64_t Nw, int M, SearchWs* ws, char* base) {
+__device__ __forceinline__ float warp_sum_f(float v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Forward + reverse LB_Keogh for few LB_Kim survivors (at most sparse_max,
+// scattered over the stream): a warp per window, lanes over the window's
+// samples (coalesced).  The forward bound first, abandoned once its running
+// sum passes the best-so-far; then, for the windows still below, the reverse
+// bound against the +-W envelope of the window's own span of the stream,
+// x[w-W, w+M-1+W] clipped to [0, N) (the values env_window_kernel computes
+// for the whole stream), built in shared memory by doubling the min/max spans
+// up to the largest power of two p <= 2W+1.  Survivors -> q2 as in
+// keogh_filter_kernel.  Shared memory: 2 * S floats per warp, S >= M + 2W.
+template <bool EU>
+__global__ void __launch_bounds__(256)
+keogh_sparse_kernel(const float* __restrict__ x, int64_t N, const double* __restrict__ mu,
+                    const float* __restrict__ sigma, const float* __restrict__ zq,
+                    const float2* __restrict__ qenv, const float* __restrict__ lbkim, int M, int W,
+                    int S, const int* __restrict__ q1, const int* __restrict__ n1p,
+                    const unsigned long long* key, Cand* __restrict__ q2, int* __restrict__ n2,
+                    int sparse_max) {
+    extern __shared__ float ksm[];
+    const int n1 = *(const volatile int*)n1p;
+    if (n1 > sparse_max) return;  // keogh_filter_kernel takes many survivors
+    const int lane = threadIdx.x & 31;
+    const int wib = threadIdx.x >> 5;
+    float* lo = ksm + (size_t)wib * 2 * S;
+    float* hi = lo + S;
+    const float lim = load_bsf(key) / kLbSlack;
+    const int K = 2 * W + 1, span = M + 2 * W;
+    int p = 1;
+    while (2 * p <= K) p *= 2;
+    const int nwarps = (gridDim.x * blockDim.x) >> 5;
+    for (int i = (int)(((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5); i < n1;
+         i += nwarps) {
+        const int w = q1[i];
+        const Norm nm = make_norm(mu[w], sigma[w]);
+        const float* __restrict__ xw = x + w;
+        // forward LB_Keogh, checked every 128 samples
+        float af = 0.f, tf = 0.f;
+        bool pruned = false;
+        for (int k0 = 0; k0 < M && !pruned; k0 += 128) {
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int k = k0 + 32 * u + lane;
+                if (k < M) {
+                    const float z = znorm(nm, __ldg(xw + k));
+                    const float2 e = __ldg(qenv + k);
+                    const float df = max3f(z - e.y, e.x - z, 0.f);
+                    af = EU ? fmaf(df, df, af) : af + df;
+                }
+            }
+            tf = warp_sum_f(af);
+            pruned = tf >= lim;
+        }
+        if (pruned) continue;
+        // the window's span of the stream, then min/max spans doubled in place
+        // (chunks in increasing order: a partner e + q > e is never rewritten
+        // before it is read)
+        for (int e = lane; e < span; e += 32) {
+            const int64_t g = (int64_t)w - W + e;
+            const bool in = g >= 0 && g < N;
+            const float v = in ? __ldg(x + g) : 0.f;
+            lo[e] = in ? v : CDTW_INF;
+            hi[e] = in ? v : -CDTW_INF;
+        }
+        __syncwarp();
+        for (int q = 1; q < p; q *= 2) {
+            for (int e0 = 0; e0 < span - q; e0 += 32) {
+                const int e = e0 + lane;
+                float a = 0.f, b = 0.f;
+                if (e < span - q) {
+                    a = fminf(lo[e], lo[e + q]);
+                    b = fmaxf(hi[e], hi[e + q]);
+                }
+                __syncwarp();
+                if (e < span - q) {
+                    lo[e] = a;
+                    hi[e] = b;
+                }
+                __syncwarp();
+            }
+        }
+        // reverse LB_Keogh: the query against the window's envelope
+        float ar = 0.f, tr = 0.f;
+        for (int k0 = 0; k0 < M && !pruned; k0 += 128) {
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int k = k0 + 32 * u + lane;
+                if (k < M) {
+                    const int c = k + K - p;
+                    const float L = fminf(lo[k], lo[c]), U = fmaxf(hi[k], hi[c]);
+                    const float qv = __ldg(zq + k);
+                    const float dr = max3f(qv - znorm(nm, U), znorm(nm, L) - qv, 0.f);
+                    ar = EU ? fmaf(dr, dr, ar) : ar + dr;
+                }
+            }
+            tr = warp_sum_f(ar);
+            pruned = tr >= lim;
+        }
+        __syncwarp();  // the span buffer is rewritten for the next window
+        if (pruned) continue;
+        const float lb = fmaxf(lbkim[w], fmaxf(tf, tr));
+        if (lane == 0 && lb < lim) {
+            Cand c;
+            c.w = w;
+            c.lb = lb;
+            c.lbk = tf;
+            q2[atomicAdd(n2, 1)] = c;
+        }
+    }
+}
+
+constexpr int kSparseSpanMax = 6144;  // M + 2W of the per-window envelope (48 KB a warp)
+
+// Forward + reverse LB_Keogh of the LB_Kim survivors q1 (count *n1, known
+// only on the device) into q2 / *n2: up to sparse_max survivors a warp per
+// window with the window's own envelope (keogh_sparse_kernel), above that the
+// stream envelope of the whole stream and a thread per window
+// (keogh_filter_kernel).  Both are launched; each returns at once outside its
+// regime, as does the stream envelope below it.
+int launch_keogh(cdtw_handle h, const float* x, int64_t N, const double* mu, const float* sigma,
+                 bool euclid, const SearchWs& ws) {
+    const QueryPack& q = h->q;
+    const int M = q.M, W = q.W;
+    const int span = M + 2 * W;
+    const int S = (int)round_up(span, 4);
+    const int sparse_max =
+        span <= kSparseSpanMax ? (int)std::min<int64_t>(N / 256, (int64_t)1 << 18) : -1;
+    CDTW_TRY(launch_stream_envelope(h, x, N, W, ws.envscratch, ws.xenv, ws.ctr + 0, sparse_max));
+    const int grid = h->sm_count * 8;
+    if (euclid)
+        keogh_filter_kernel<true><<<grid, 256, 0, h->stream>>>(
+            x, mu, sigma, q.zq, q.env, ws.xenv, ws.lbkim, M, ws.q1, ws.ctr + 0, ws.key, ws.q2,
+            ws.ctr + 1, sparse_max);
+    else
+        keogh_filter_kernel<false><<<grid, 256, 0, h->stream>>>(
+            x, mu, sigma, q.zq, q.env, ws.xenv, ws.lbkim, M, ws.q1, ws.ctr + 0, ws.key, ws.q2,
+            ws.ctr + 1, sparse_max);
+    CDTW_LAUNCH(h, "keogh_filter_kernel");
+    if (sparse_max <= 0) return CDTW_OK;
+    const int wpb = (int)std::max<int64_t>(
+        1, std::min<int64_t>(8, (int64_t)(200 * 1024) / ((int64_t)8 * S)));
+    const size_t smem = (size_t)wpb * 2 * S * sizeof(float);
+    auto k = euclid ? keogh_sparse_kernel<true> : keogh_sparse_kernel<false>;
+    CDTW_CUDA(h, cudaFuncSetAttribute((const void*)k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)smem));
+    int per_sm = 0;
+    CDTW_CUDA(h, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)k, 32 * wpb,
+                                                               smem));
+    const int64_t blocks = std::max<int64_t>(
+        1, std::min<int64_t>(div_up(sparse_max, wpb), (int64_t)std::max(per_sm, 1) * h->sm_count));
+    k<<<(unsigned)blocks, 32 * wpb, smem, h->stream>>>(x, N, mu, sigma, q.zq, q.env, ws.lbkim, M,
+                                                       W, S, ws.q1, ws.ctr + 0, ws.key, ws.q2,
+                                                       ws.ctr + 1, sparse_max);
+    CDTW_LAUNCH(h, "keogh_sparse_kernel");
+    return CDTW_OK;
+}
+
+// The survivors of the bounds run as pairwise wavefronts (at most
+// kWaveSurvivors of them) when the band fits the pairwise forward and a
+// window has at least kWaveMinCells band cells: a thread per window is then
+// latency-bound.
+bool wave_eligible(int M, int W) {
+    const int Wp = std::min(W, M - 1);
+    const double wcells = (double)M * (2.0 * Wp + 1.0) - (double)Wp * (Wp + 1.0);
+    return Wp <= CDTW_PAIR_MAX_BAND && M <= CDTW_MAX_QUERY && wcells >= kWaveMinCells;
+}
+
+size_t carve_search(int64_t N, int64_t Nw, int M, int W, SearchWs* ws, char* base) {
     size_t off = 0;
     auto take = [&](size_t bytes) {
         const size_t o = off;
@@ -216,6 +402,7 @@ size_t carve_search(int64_t N, int64_t Nw, int M, SearchWs* ws, char* base) {
     const int64_t nblk = div_up(Nw, kKimBlock);
     ws->lbkim = (float*)take(sizeof(float) * Nw);
     ws->seeds = (unsigned long long*)take(sizeof(unsigned long long) * nblk);
+    ws->bmax = (unsigned*)take(sizeof(unsigned) * nblk);
     ws->seed_cands = (Cand*)take(sizeof(Cand) * nblk);
     ws->q1 = (int*)take(sizeof(int) * Nw);
     ws->q2 = (Cand*)take(sizeof(Cand) * Nw);
@@ -223,9 +410,12 @@ size_t carve_search(int64_t N, int64_t Nw, int M, SearchWs* ws, char* base) {
     ws->envscratch = (float*)take(stream_envelope_scratch_bytes(N));
     ws->ctr = (int*)take(sizeof(int) * 8);
     ws->key = (unsigned long long*)take(sizeof(unsigned long long));
-    // rows of the seed windows (at most kSeedMax) and of the survivors run as
+    // rows of the seed windows (at most one per LB_Kim block, kSeedMax) and,
+    // when that pass can run for this (M, W), of the survivors run as
     // wavefronts (at most kWaveSurvivors)
-    const int64_t rows = std::min<int64_t>(Nw, std::max<int64_t>(kSeedMax, kWaveSurvivors));
+    const int64_t rows = wave_eligible(M, W)
+                             ? std::min<int64_t>(Nw, std::max<int64_t>(kSeedMax, kWaveSurvivors))
+                             : std::min<int64_t>(nblk, kSeedMax);
     ws->seed_cap = std::min<int64_t>(rows * M, kSeedZMax);
     ws->seed_z = (float*)take(sizeof(float) * ws->seed_cap);
     ws->seed_d = (float*)take(sizeof(float) * std::max(kSeedMax, kWaveSurvivors));
@@ -274,9 +464,9 @@ struct TopkWs {
     int* nh;
 };
 
-size_t carve_topk(int64_t N, int64_t Nw, int M, int64_t cap, SearchWs* sw, TopkWs* tw,
+size_t carve_topk(int64_t N, int64_t Nw, int M, int W, int64_t cap, SearchWs* sw, TopkWs* tw,
                   char* base) {
-    size_t off = carve_search(N, Nw, M, sw, base);
+    size_t off = carve_search(N, Nw, M, W, sw, base);
     auto take = [&](size_t bytes) {
         const size_t o = off;
         off = (size_t)round_up((int64_t)(off + bytes), 256);
@@ -296,11 +486,11 @@ int64_t topk_cap(int64_t Nw) { return std::min<int64_t>(Nw, (int64_t)1 << 24); }
 
 }  // namespace
 
-size_t topk_workspace_bytes(int64_t N, int M) {
+size_t topk_workspace_bytes(int64_t N, int M, int W) {
     SearchWs sw;
     TopkWs tw;
     const int64_t Nw = N - M + 1;
-    return carve_topk(N, Nw, M, topk_cap(Nw), &sw, &tw, nullptr);
+    return carve_topk(N, Nw, M, W, topk_cap(Nw), &sw, &tw, nullptr);
 }
 
 // Greedy non-overlapping selection over the (distance, window) keys in
@@ -344,10 +534,11 @@ int run_topk(cdtw_handle h, const float* x, int64_t N, const double* mu, const f
     SearchWs ws;
     TopkWs tw;
     const int64_t cap = topk_cap(Nw);
-    carve_topk(N, Nw, M, cap, &ws, &tw, ws_base);
+    carve_topk(N, Nw, M, q.W, cap, &ws, &tw, ws_base);
     const int nseg = (int)div_up(Nw, 2 * (int64_t)M);
     // 1. LB_Kim of every window, seeds per segment, their exact cDTW
-    CDTW_TRY(launch_lb_kim(h, x, N, mu, sigma, nullptr, Nw, euclid, ws.lbkim, ws.seeds));
+    CDTW_TRY(launch_lb_kim(h, x, N, mu, sigma, nullptr, Nw, euclid, ws.lbkim, ws.seeds,
+                           ws.bmax));
     topk_seed_kernel<<<(unsigned)div_up((int64_t)nseg * 32, 256), 256, 0, h->stream>>>(
         ws.lbkim, (int)Nw, M, nseg, tw.sidx);
     CDTW_LAUNCH(h, "topk_seed_kernel");
@@ -369,16 +560,7 @@ int run_topk(cdtw_handle h, const float* x, int64_t N, const double* mu, const f
     const int grid = h->sm_count * 8;
     compact_kim_kernel<<<grid, 256, 0, h->stream>>>(ws.lbkim, (int)Nw, ws.key, ws.q1, ws.ctr + 0);
     CDTW_LAUNCH(h, "compact_kim_kernel");
-    CDTW_TRY(launch_stream_envelope(h, x, N, q.W, ws.envscratch, ws.xenv));
-    if (euclid)
-        keogh_filter_kernel<true><<<grid, 256, 0, h->stream>>>(
-            x, mu, sigma, q.zq, q.env, ws.xenv, ws.lbkim, M, ws.q1, ws.ctr + 0, ws.key, ws.q2,
-            ws.ctr + 1);
-    else
-        keogh_filter_kernel<false><<<grid, 256, 0, h->stream>>>(
-            x, mu, sigma, q.zq, q.env, ws.xenv, ws.lbkim, M, ws.q1, ws.ctr + 0, ws.key, ws.q2,
-            ws.ctr + 1);
-    CDTW_LAUNCH(h, "keogh_filter_kernel");
+    CDTW_TRY(launch_keogh(h, x, N, mu, sigma, euclid, ws));
     int cnt[2];
     CDTW_CUDA(h, cudaMemcpyAsync(cnt, ws.ctr, sizeof(cnt), cudaMemcpyDeviceToHost, h->stream));
     CDTW_CUDA(h, cudaStreamSynchronize(h->stream));
@@ -412,9 +594,9 @@ int run_topk(cdtw_handle h, const float* x, int64_t N, const double* mu, const f
     return CDTW_OK;
 }
 
-size_t search_workspace_bytes(int64_t N, int M) {
+size_t search_workspace_bytes(int64_t N, int M, int W) {
     SearchWs ws;
-    return carve_search(N, N - M + 1, M, &ws, nullptr);
+    return carve_search(N, N - M + 1, M, W, &ws, nullptr);
 }
 
 // Runs the whole pruned search; the result key and the stage counts stay on
@@ -424,17 +606,18 @@ int run_search(cdtw_handle h, const float* x, int64_t N, const double* mu, const
     const QueryPack& q = h->q;
     const int64_t Nw = N - q.M + 1;
     SearchWs ws;
-    carve_search(N, Nw, q.M, &ws, ws_base);
+    carve_search(N, Nw, q.M, q.W, &ws, ws_base);
     CDTW_CUDA(h, cudaMemsetAsync(ws.ctr, 0, sizeof(int) * 8, h->stream));
     CDTW_CUDA(h, cudaMemsetAsync(ws.key, 0xff, sizeof(unsigned long long), h->stream));
     // 1. LB_Kim of every window + per-block seeds
     const int64_t nblk = div_up(Nw, kKimBlock);
-    CDTW_TRY(launch_lb_kim(h, x, N, mu, sigma, nullptr, Nw, euclid, ws.lbkim, ws.seeds));
+    CDTW_TRY(launch_lb_kim(h, x, N, mu, sigma, nullptr, Nw, euclid, ws.lbkim, ws.seeds,
+                           ws.bmax));
     // 2. cDTW of the seeds
     const int G = (int)std::max<int64_t>(1, div_up(nblk, seed_target(q.M, q.W)));
     const int nseed = (int)div_up(nblk, G);
     seeds_to_cands_kernel<<<(unsigned)div_up(nseed, 256), 256, 0, h->stream>>>(
-        ws.seeds, (int)nblk, G, ws.seed_cands, ws.ctr + 4);
+        ws.seeds, ws.bmax, (int)nblk, G, ws.seed_cands, ws.ctr + 4, (unsigned*)ws.ctr + 5);
     CDTW_LAUNCH(h, "seeds_to_cands_kernel");
     // the seeds only bound the search from above, so their cDTW runs as
     // pairwise wavefronts (a lane group per seed: low latency with few
@@ -459,23 +642,12 @@ int run_search(cdtw_handle h, const float* x, int64_t N, const double* mu, const
     compact_kim_kernel<<<grid, 256, 0, h->stream>>>(ws.lbkim, (int)Nw, ws.key, ws.q1, ws.ctr + 0);
     CDTW_LAUNCH(h, "compact_kim_kernel");
     // 4. LB_Keogh forward + reverse
-    CDTW_TRY(launch_stream_envelope(h, x, N, q.W, ws.envscratch, ws.xenv));
-    if (euclid)
-        keogh_filter_kernel<true><<<grid, 256, 0, h->stream>>>(
-            x, mu, sigma, q.zq, q.env, ws.xenv, ws.lbkim, q.M, ws.q1, ws.ctr + 0, ws.key, ws.q2,
-            ws.ctr + 1);
-    else
-        keogh_filter_kernel<false><<<grid, 256, 0, h->stream>>>(
-            x, mu, sigma, q.zq, q.env, ws.xenv, ws.lbkim, q.M, ws.q1, ws.ctr + 0, ws.key, ws.q2,
-            ws.ctr + 1);
-    CDTW_LAUNCH(h, "keogh_filter_kernel");
+    CDTW_TRY(launch_keogh(h, x, N, mu, sigma, euclid, ws));
     // 5. cDTW of the survivors: as pairwise wavefronts when at most `wcap`
     //    remain and a window is long enough that a thread per window is
     //    latency-bound, else with early abandoning
     const int wcap = (int)std::min<int64_t>(kWaveSurvivors, ws.seed_cap / q.M);
-    const double wcells = (double)q.M * (2.0 * Wp + 1.0) - (double)Wp * (Wp + 1.0);
-    if (Wp <= CDTW_PAIR_MAX_BAND && q.M <= CDTW_MAX_QUERY && wcap >= 32 &&
-        wcells >= kWaveMinCells) {
+    if (wave_eligible(q.M, q.W) && wcap >= 32) {
         wave_gather_kernel<<<(unsigned)div_up((int64_t)wcap * 32, 256), 256, 0, h->stream>>>(
             x, mu, sigma, ws.q2, ws.ctr + 1, wcap, q.M, ws.seed_z, ws.ctr + 3);
         CDTW_LAUNCH(h, "wave_gather_kernel");

@@ -77,7 +77,9 @@ int main(int argc, char* argv[]) {
     const double ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
     std::cout << "Location: " << loc << std::endl;
     std::cout << "Distance: " << dist << std::endl;
-    std::cout << 1 << std::endl;
+    int flag = 0;
+    cdtw_search_flag(h, &flag);  // (best < largest LB_Kim), include/cdtw.cuh:585
+    std::cout << flag << std::endl;
     std::cout << "Miliseconds to find best match: " << ms << std::endl;
     if (json) {
         int64_t c[3];

@@ -17,6 +17,7 @@
 #ifndef CUDADTW_H
 #define CUDADTW_H
 
+#include <stddef.h>
 #include <stdint.h>
 
 #ifdef __cplusplus
@@ -58,6 +59,15 @@ int cdtw_destroy(cdtw_handle h);
 int cdtw_set_stream(cdtw_handle h, void* cuda_stream);
 const char* cdtw_last_error(cdtw_handle h);
 const char* cdtw_status_string(int status);
+
+/* Cap the device memory this handle holds (its grow-only work area, query
+ * pack, strip rings, cached batched-search plan, and the per-call memory of
+ * cdtw_refine_templates) at `bytes`; 0 removes the cap.  A call that would
+ * need more fails with CDTW_ENOMEM before allocating, and the handle stays
+ * usable for smaller calls.  No reference counterpart (prune_cdtw allocates
+ * its temporaries unchecked and exits on failure, include/cdtw.cuh:521-525
+ * with CUERR of include/cuda_def.cuh:6-8). */
+int cdtw_set_memory_limit(cdtw_handle h, size_t bytes);
 
 /* W = M*(P*0.01), truncated: GPU-dtw.cu:27 / GPU-ldtw.cu:412. */
 int cdtw_band_from_percent(int M, int P);
@@ -153,6 +163,15 @@ int cdtw_search_host(cdtw_handle h, const float* h_query, int M, const float* h_
  * pruning percentages, UCR_DTW_BIN.cpp:738-741). */
 int cdtw_search_counts(cdtw_handle h, int64_t* counts);
 
+/* The line GPU-DTW prints after "Distance:" for the last search on this
+ * handle: 1 when its best distance (squared for CDTW_EUCLIDEAN) lies below
+ * the largest LB_Kim of any window, else 0.  prune_cdtw prints
+ * (best_cdtw < max_kim) (include/cdtw.cuh:585), max_kim being LB_Kim at the
+ * end of the ascending LB_Kim order it has searched (:541, :572); it stops
+ * early only when best_cdtw < max_kim, and otherwise reaches the end of the
+ * order, where max_kim is the largest LB_Kim of all, so the two agree. */
+int cdtw_search_flag(cdtw_handle h, int* flag);
+
 /* ---- batched search ------------------------------------------------------------- */
 
 /* Best match of each of nq queries (lengths Ms[q] in [11, 4096], bands Ws[q];
@@ -230,8 +249,11 @@ int ldtw_search_host(cdtw_handle h, const float* h_query, int M, const float* h_
  * Limits: M <= CDTW_NOALLOC_MAX_QUERY, N-M+1 <= CDTW_NOALLOC_MAX_WINDOWS,
  * band W <= 40 (after clamping W to M-1); larger requests return
  * CDTW_EUNSUPPORTED with the reason in errbuf (errlen bytes, may be NULL/0).
- * The first call on a device looks up the array's address on that device;
- * make that first call before any stream capture.  All calls on a device
+ * The first call on a device looks up the array's address on that device
+ * (and again after the device's context was torn down and re-created, e.g.
+ * by cudaDeviceReset); make that first call before any stream capture.  The
+ * array's memory is reserved when the CUDA runtime loads this library's
+ * device code, not by the call.  All calls on a device
  * share the one array: calls whose work overlaps on the GPU (different
  * streams, or host threads without ordering) race and corrupt each other's
  * results; order them on one stream. */
@@ -298,10 +320,13 @@ int cdtw_refine_templates(cdtw_handle h, const float* d_subject, int64_t N, floa
 /* ---- kernel selection ----------------------------------------------------------- */
 
 enum cdtw_variant {
-    CDTW_VARIANT_AUTO = 0,      /* built-in rule: register band for W <= 96, else 16-row strips */
+    CDTW_VARIANT_AUTO = 0,      /* built-in rule: register band for W <= 96, lane groups up
+                                   to W = 767, 16-row strips above                      */
     CDTW_VARIANT_REGISTER = 1,  /* one thread per window, the band in registers (W <= 96) */
     CDTW_VARIANT_STRIP16 = 2,   /* strips of 16 rows, boundary ring (W >= 15)            */
-    CDTW_VARIANT_STRIP32 = 3    /* strips of 32 rows, boundary ring (W >= 31)            */
+    CDTW_VARIANT_STRIP32 = 3,   /* strips of 32 rows, boundary ring (W >= 31)            */
+    CDTW_VARIANT_LANE = 4       /* band spread over a lane group, two windows per group
+                                   (27 <= W <= 767)                                     */
 };
 
 /* Kernel variant for bands w_lo..w_hi on this handle (what the autotuner,

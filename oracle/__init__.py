@@ -32,11 +32,15 @@ _int = ctypes.c_int
 
 
 def build() -> None:
+    """Builds liboracle.so and, when the reference tree is present (its root
+    in the CDTW_REFERENCE_DIR environment variable), the reference's UCR Suite
+    binaries into _ref/ (kept when already built)."""
     subprocess.run(["make", "-s", "-C", HERE, "all"], check=True)
-    if os.path.isdir("/root/reference") and not (
+    refdir = os.environ.get("CDTW_REFERENCE_DIR", "")
+    if refdir and os.path.isdir(refdir) and not (
             os.path.exists(os.path.join(REF_DIR, "UCR_DTW_BIN"))
             and os.path.exists(os.path.join(REF_DIR, "UCR_ED_BIN"))):
-        subprocess.run(["make", "-s", "-C", HERE, "ref"], check=True)
+        subprocess.run(["make", "-s", "-C", HERE, "ref", f"REFDIR={refdir}"], check=True)
 
 
 def lib():
@@ -209,7 +213,8 @@ def _run_ucr(binary: str, args: list[str]):
     if not os.path.exists(path):
         raise FileNotFoundError(f"{path} missing: run `make -C oracle ref` where the "
                                 "reference sources are available")
-    out = subprocess.run([path] + args, check=True, capture_output=True, text=True).stdout
+    out = subprocess.run([path] + args, check=True, stdout=subprocess.PIPE,
+                         stderr=subprocess.DEVNULL, text=True).stdout
     loc = int(_LOC.search(out).group(1))
     dist = float(_DIST.search(out).group(1))
     tm = _TIME.search(out)
@@ -225,6 +230,77 @@ def ucr_dtw(x: np.ndarray, q: np.ndarray, r_arg: str):
         x.astype(np.float64).tofile(xp)
         q.astype(np.float64).tofile(qp)
         return _run_ucr("UCR_DTW_BIN", [xp, qp, str(q.size), r_arg, str(x.size)])
+
+
+def ucr_band_arg(w: int, m: int) -> str:
+    """UCR_DTW_BIN's R argument for an absolute band w: R > 1 is taken as the
+    band itself (UCR_DTW_BIN.cpp:420-423); w <= 1 is passed as the fraction
+    w / m, which UCR floors back to w."""
+    if w > 1:
+        return str(int(w))
+    return repr((w + 0.5) / m) if w == 1 else "0"
+
+
+class UcrShards:
+    """UCR_DTW_BIN over `shards` concurrent processes on one stream: shard s
+    covers its share of the windows of the longest query `max_m` plus the
+    samples that follow (the halo), written once as exact FP64 widenings of
+    the float32 samples.  ``search(q, w)`` runs every shard on its windows
+    (UCR reads only the n samples it is given) and combines the shard results
+    by the FP64 oracle's distance at each shard's location, lowest location
+    on ties (UCR prints 6 significant digits).  Use as a context manager."""
+
+    def __init__(self, x: np.ndarray, shards: int | None = None, max_m: int = 8192):
+        self.x = x
+        self.path = os.path.join(REF_DIR, "UCR_DTW_BIN")
+        if not os.path.exists(self.path):
+            raise FileNotFoundError(f"{self.path} missing: run `make -C oracle ref`")
+        self.shards = max(1, min(shards or (os.cpu_count() or 1), x.size))
+        self.bounds = [x.size * s // self.shards for s in range(self.shards + 1)]
+        self.dir = tempfile.TemporaryDirectory()
+        self.files = []
+        for s in range(self.shards):
+            a = self.bounds[s]
+            fp = os.path.join(self.dir.name, f"data{s}.f64")
+            x[a:min(x.size, self.bounds[s + 1] + max_m - 1)].astype(np.float64).tofile(fp)
+            self.files.append(fp)
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.dir.cleanup()
+
+    def search(self, q: np.ndarray, w: int):
+        """Returns (location, distance as UCR printed it, wall seconds,
+        [per-shard clock() seconds])."""
+        import time
+        m = q.size
+        nw = self.x.size - m + 1
+        qp = os.path.join(self.dir.name, "query.f64")
+        q.astype(np.float64).tofile(qp)
+        jobs = []
+        for s in range(self.shards):
+            a, b = self.bounds[s], min(self.bounds[s + 1], nw)
+            if b > a:
+                jobs.append((a, self.files[s], b - a + m - 1))
+        t0 = time.perf_counter()
+        procs = [subprocess.Popen([self.path, fp, qp, str(m), ucr_band_arg(w, m), str(n)],
+                                  stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                 for _, fp, n in jobs]
+        outs = [p.communicate()[0] for p in procs]
+        wall = time.perf_counter() - t0
+        if any(p.returncode != 0 for p in procs):
+            raise RuntimeError("UCR_DTW_BIN failed on a shard")
+        locs, dists, cpus = [], [], []
+        for (a, _, _), out in zip(jobs, outs):
+            locs.append(a + int(_LOC.search(out).group(1)))
+            dists.append(float(_DIST.search(out).group(1)))
+            tm = _TIME.search(out)
+            cpus.append(float(tm.group(1)) if tm else None)
+        exact = cdtw_list(q, self.x, w, np.array(locs, dtype=np.int64))
+        best = min(range(len(jobs)), key=lambda s: (exact[s], locs[s]))
+        return locs[best], dists[best], wall, cpus
 
 
 def ucr_ed(x: np.ndarray, q: np.ndarray):

@@ -19,8 +19,11 @@ def test_candidates_respect_kernel_limits():
     assert all(r != 0 for r, _ in at.batched_candidates(97))
     assert all(r <= 8 for r, _ in at.batched_candidates(7))
     assert at.variant_candidates(10) == ["register"]
-    assert at.variant_candidates(40) == ["register", "strip16", "strip32"]
-    assert at.variant_candidates(200) == ["strip16", "strip32"]
+    assert at.variant_candidates(40) == ["register", "strip16", "strip32", "lane"]
+    assert at.variant_candidates(200) == ["strip16", "strip32", "lane"]
+    assert at.variant_candidates(800) == ["strip16", "strip32"]
+    assert at.variant_candidates(384) == ["strip16", "strip32"]  # no lane shape fits
+    assert at.lane_shape(204) == (16, 26) and at.lane_shape(409) == (32, 26)
 
 
 def test_tune_picks_fastest_and_maps_queries(tmp_path):
@@ -48,5 +51,8 @@ def test_tune_picks_fastest_and_maps_queries(tmp_path):
 
 def test_tune_variants_fake():
     v = at.tune_variants([10, 50, 200], lambda w, var: {"register": 3, "strip16": 2,
-                                                          "strip32": 1}[var] if w > 40 else 1)
+                                                          "strip32": 1, "lane": 1.5}[var]
+                         if w > 40 else 1)
     assert v == {"10": "register", "50": "strip32", "200": "strip32"}
+    v = at.tune_variants([200], lambda w, var: {"strip16": 2, "strip32": 3, "lane": 1}[var])
+    assert v == {"200": "lane"}

@@ -50,6 +50,27 @@ def test_batched_equals_single_query_search(handle):
     _check(handle, dx, qs2, ws, locs2, dists2)
 
 
+@pytest.mark.parametrize("metric", [0, 1])
+def test_batched_matches_fp64_oracle(handle, metric):
+    """Anchor independent of the plain CUDA path: every query's location is
+    the FP64 oracle's argmin over all windows (or ties with it at 1e-5
+    relative), its distance within 1e-4 of the oracle at that window."""
+    import oracle
+    x = synth.ecg_like(40_000, seed=41)
+    batch = synth.batch_queries(x, 12, seed=8, m_lo=64, m_hi=200)
+    qs = [b[0] for b in batch]
+    ws = [b[1] for b in batch]
+    dx = torch.from_numpy(x).cuda()
+    locs, dists = handle.search_batched(dx, qs, ws, metric=metric)
+    eu = metric == 0
+    for q, w, loc, dist in zip(qs, ws, locs, dists):
+        ref = oracle.cdtw_all(q, x, w, euclid=eu)
+        v = np.sqrt(ref) if eu else ref
+        best, _ = oracle.argmin(ref)
+        assert abs(v[loc] - v[best]) <= 1e-5 * v[best]
+        assert abs(dist - v[loc]) <= 1e-4 * v[loc]
+
+
 @pytest.mark.parametrize("rows", [0, 1, 2, 4, 8, 16])
 def test_batched_every_strip_height(handle, rows):
     """rows = 0: register-band main pass; 1..16: strips of that height."""

@@ -132,7 +132,8 @@ def test_errors_are_status_codes(handle):
                                       (300, 63, 2000), (512, 102, 1500), (1024, 204, 600),
                                       (2048, 409, 200), (777, 300, 300)])
 def test_all_windows_wide_bands(handle, m, w, nwin):
-    """Bands above the register-band limit run on the strip kernel."""
+    """Bands above the register-band limit: the lane-group kernel (the
+    strip kernel where no lane shape fits)."""
     x = synth.metal_like(m + nwin - 1, seed=w)
     q, _ = synth.cut_query(x, m, seed=w, noise=0.2)
     got = _all_windows(handle, q, x, w)
@@ -141,16 +142,64 @@ def test_all_windows_wide_bands(handle, m, w, nwin):
     np.testing.assert_allclose(got1, oracle.cdtw_all(q, x, w, euclid=False), rtol=RTOL, atol=ATOL)
 
 
+@pytest.mark.parametrize("m,w", [(200, 27), (300, 60), (400, 96), (260, 97), (700, 150),
+                                 (1024, 204), (1100, 383), (1500, 384), (2048, 409),
+                                 (1600, 767)])
+def test_all_windows_variants_bit_identical(handle, m, w):
+    """The lane-group kernel (band over a group of lanes, two windows per
+    group), the strip kernels and the register band compute every cell with
+    the same operations: their all-windows outputs are bit-identical, for
+    both costs, across lane shapes (4 to 32 lanes of 18 to 48 cells) and at
+    the bands no lane shape fits (384), and stay within 1e-4 of the oracle."""
+    from cudadtw_b200 import autotune as at
+    nwin = 700
+    x = synth.metal_like(m + nwin - 1, seed=m + w)
+    q, _ = synth.cut_query(x, m, seed=w, noise=0.2)
+    dx = _dev(x)
+    avg, std = handle.avg_std(dx, m)
+    handle.set_query(q, w)
+    variants = ["strip16"] + (["register"] if w <= 96 else []) + \
+        (["lane"] if at.lane_shape(w) else [])
+    for metric in (0, 1):
+        outs = {}
+        for v in variants:
+            handle.set_band_variant(w, w, v)
+            outs[v] = handle.gpu_cdtw(dx, avg, std, metric=metric).cpu().numpy()
+        handle.set_band_variant(w, w, "auto")
+        auto = handle.gpu_cdtw(dx, avg, std, metric=metric).cpu().numpy()
+        for v in variants:
+            np.testing.assert_array_equal(outs[v], auto, err_msg=v)
+        ref = oracle.cdtw_all(q, x, w, euclid=(metric == 0))
+        np.testing.assert_allclose(auto.astype(np.float64), ref, rtol=RTOL, atol=ATOL)
+
+
+def test_lane_kernel_index_list(handle):
+    x = synth.ecg_like(20000, seed=15)
+    q, _ = synth.cut_query(x, 512, seed=15, noise=0.05)
+    dx = _dev(x)
+    avg, std = handle.avg_std(dx, 512)
+    handle.set_query(q, 150)
+    idx = np.random.default_rng(3).permutation(x.size - 511)[:501].astype(np.int32)
+    idx[8] = -3  # outside the subject: NaN, no access
+    got = handle.gpu_cdtw(dx, avg, std, indices=_dev(idx)).cpu().numpy()
+    full = handle.gpu_cdtw(dx, avg, std).cpu().numpy()
+    assert np.isnan(got[8])
+    keep = np.arange(idx.size) != 8
+    np.testing.assert_array_equal(got[keep], full[idx[keep]])
+
+
 def test_strip_kernel_index_list(handle):
     x = synth.ecg_like(20000, seed=5)
     q, _ = synth.cut_query(x, 512, seed=5, noise=0.05)
     dx = _dev(x)
     avg, std = handle.avg_std(dx, 512)
     handle.set_query(q, 102)
+    handle.set_band_variant(102, 102, "strip16")
     idx = np.random.default_rng(1).permutation(x.size - 511)[:500].astype(np.int32)
     idx[7] = x.size  # outside the subject: NaN, no access
     got = handle.gpu_cdtw(dx, avg, std, indices=_dev(idx)).cpu().numpy()
     full = handle.gpu_cdtw(dx, avg, std).cpu().numpy()
+    handle.set_band_variant(102, 102, "auto")
     assert np.isnan(got[7])
     keep = np.arange(idx.size) != 7
     np.testing.assert_array_equal(got[keep], full[idx[keep]])

@@ -87,6 +87,10 @@ def test_gpu_dtw_driver_matches_ucr(tmp_path, golden):
         dist = float(re.search(r"Distance: ([0-9.eE+-]+)", r.stdout).group(1))
         assert "best match:" in r.stdout  # the line results/benchCDTW.py parses
         assert loc == c["ucr_location"], c["name"]
+        # the termination flag printed after the distance (cdtw.cuh:585):
+        # squared best < largest LB_Kim (FP64 oracle)
+        flag = int(re.search(r"Distance: [^\n]*\n(\d)\n", r.stdout).group(1))
+        assert flag == int(dist * dist < oracle.lb_kim(q, x).max())
         assert abs(dist - c["ucr_distance"]) <= 1e-4 * c["ucr_distance"]
 
 

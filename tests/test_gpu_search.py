@@ -106,9 +106,57 @@ def test_search_equals_unpruned_argmin(handle, kind, m, p):
         assert dist == np.float32(np.sqrt(best) if metric == 0 else best)
         nw, nkim, ndtw = handle.search_counts()
         assert nw == x.size - m + 1 and 0 < ndtw <= nkim <= nw
+        # the reference's termination flag (cdtw.cuh:585): best < largest LB_Kim
+        kim = handle.lb_kim(dx, avg, std, metric=metric).cpu().numpy()
+        assert handle.search_flag() == int(np.float32(best) < kim.max())
         ref = oracle.cdtw_list(q, x, w, np.array([loc]), euclid=(metric == 0))[0]
         ref = np.sqrt(ref) if metric == 0 else ref
         assert abs(dist - ref) <= 1e-4 * ref
+
+
+@pytest.mark.parametrize("kind,m,p,noise", [("metal", 1024, 20, 1.0), ("walk", 800, 20, 1.0)])
+def test_search_wavefront_survivor_range(handle, kind, m, p, noise):
+    """Cases whose bound survivors (about 1.1-1.4 thousand by the FP64
+    oracle's bounds against the best distance) fall in the range that runs as
+    pairwise wavefronts (more than 512, at most 8192, with at least 4e4 band
+    cells per window): location and distance equal the unpruned argmin's."""
+    x = {"metal": synth.metal_like,
+         "walk": lambda n, seed: synth.random_walk(n, seed)}[kind](60000, seed=m + p)
+    q, _ = synth.cut_query(x, m, seed=p, noise=noise)
+    w = synth.band_from_percent(m, p)
+    assert m * (2 * w + 1) - w * (w + 1) >= 4e4
+    for metric in (0, 1):
+        dx, avg, std = _prep(handle, q, x, w)
+        loc, dist = handle.prune_cdtw(dx, avg, std, metric=metric)
+        allw = handle.gpu_cdtw(dx, avg, std, metric=metric).cpu().numpy()
+        assert loc == int(np.argmin(allw))
+        best = allw.min()
+        assert dist == np.float32(np.sqrt(best) if metric == 0 else best)
+        if metric == 0:
+            _, _, ndtw = handle.search_counts()
+            assert 512 < ndtw <= 8192, ndtw
+
+
+@pytest.mark.parametrize("m,p", [(700, 20), (1024, 10), (300, 50)])
+def test_search_variants_agree(handle, m, p):
+    """ECG-like streams with a noisy query: tens of thousands of windows
+    survive the bounds, so the survivors run on the early-abandoning kernels
+    (lane groups, or the strips): every variant gives the unpruned argmin."""
+    x = synth.ecg_like(40000, seed=m + p)
+    q, _ = synth.cut_query(x, m, seed=p, noise=0.3)
+    w = synth.band_from_percent(m, p)
+    dx, avg, std = _prep(handle, q, x, w)
+    for metric in (0, 1):
+        allw = handle.gpu_cdtw(dx, avg, std, metric=metric).cpu().numpy()
+        best = allw.min()
+        want = (int(np.argmin(allw)), np.float32(np.sqrt(best) if metric == 0 else best))
+        for v in ("lane", "strip16", "strip32"):
+            handle.set_band_variant(w, w, v)
+            loc, dist = handle.prune_cdtw(dx, avg, std, metric=metric)
+            assert (loc, dist) == want, v
+        handle.set_band_variant(w, w, "auto")
+        _, _, ndtw = handle.search_counts()
+        assert ndtw > 8192
 
 
 def test_search_host_path_and_ties(handle):
