@@ -36,6 +36,9 @@ SIGNATURES = {
     "cdtw_search_counts": (c_int, [c_vp, c_i64p]),
     "cdtw_search_flag": (c_int, [c_vp, ctypes.POINTER(c_int)]),
     "cdtw_set_memory_limit": (c_int, [c_vp, ctypes.c_size_t]),
+    "cdtw_stream_begin": (c_int, [c_vp, c_vp, c_int, c_int, c_int, c_i64]),
+    "cdtw_stream_push": (c_int, [c_vp, c_vp, c_i64]),
+    "cdtw_stream_end": (c_int, [c_vp, c_i64p, c_f32p, c_i64p]),
     "cdtw_topk": (c_int, [c_vp, c_vp, c_i64, c_vp, c_vp, c_int, c_int, c_vp, c_vp,
                           ctypes.POINTER(c_int)]),
     "cdtw_set_band_variant": (c_int, [c_vp, c_int, c_int, c_int]),
@@ -45,6 +48,9 @@ SIGNATURES = {
     "ed_search_host": (c_int, [c_vp, c_vp, c_int, c_vp, c_i64, c_i64p, c_f64p]),
     "ldtw_all_windows": (c_int, [c_vp, c_vp, c_i64, c_int, c_vp]),
     "ldtw_search_host": (c_int, [c_vp, c_vp, c_int, c_vp, c_i64, c_int, c_int, c_i64p, c_f64p]),
+    "ldtw_ref_all_windows": (c_int, [c_vp, c_vp, c_i64, c_int, c_int, c_vp]),
+    "ldtw_ref_search_host": (c_int, [c_vp, c_vp, c_int, c_vp, c_i64, c_int, c_int, c_int, c_i64p,
+                                     c_f32p]),
     "cdtw_all_windows_noalloc": (c_int, [c_vp, c_int, c_vp, c_i64, c_int, c_int, c_vp, c_vp,
                                          ctypes.c_char_p, c_int]),
     "cdtw_pair_path_bytes": (ctypes.c_size_t, [c_i64, c_int]),

@@ -210,6 +210,26 @@ class Handle:
                                         _ptr(dists), ctypes.byref(found)))
         return locs[:found.value], dists[:found.value]
 
+    # -- search over a stream pushed in pieces ------------------------------
+    def stream_begin(self, query, W: int, metric=EUCLIDEAN, chunk: int = 0) -> None:
+        """Start a search whose subject arrives by stream_push (chunked copies
+        overlapping the search of the previous chunk; UCR's EPOCH loop)."""
+        q = np.ascontiguousarray(query, dtype=np.float32)
+        self._check(self._lib.cdtw_stream_begin(self._h, _ptr(q), q.size, W, _metric(metric),
+                                                int(chunk)))
+        self.M, self.W = q.size, min(W, q.size - 1)
+
+    def stream_push(self, samples) -> None:
+        s = np.ascontiguousarray(samples, dtype=np.float32)
+        self._check(self._lib.cdtw_stream_push(self._h, _ptr(s), s.size))
+
+    def stream_end(self):
+        """(location, distance, samples scanned) of the whole stream."""
+        loc, dist, n = ctypes.c_int64(), ctypes.c_float(), ctypes.c_int64()
+        self._check(self._lib.cdtw_stream_end(self._h, ctypes.byref(loc), ctypes.byref(dist),
+                                              ctypes.byref(n)))
+        return loc.value, dist.value, n.value
+
     def set_memory_limit(self, nbytes: int) -> None:
         """Cap the device memory the handle holds (0: no cap); calls that
         would need more raise CudaDTWError with status CDTW_ENOMEM (2)."""
@@ -264,6 +284,26 @@ class Handle:
         self._check(self._lib.ldtw_search_host(self._h, _ptr(q), q.size, _ptr(s), s.size, W,
                                                _metric(metric), ctypes.byref(loc),
                                                ctypes.byref(dist)))
+        self.M, self.W = q.size, min(W, q.size - 1)
+        return loc.value, dist.value
+
+    def ldtw_ref_all_windows(self, subject, metric=EUCLIDEAN, znorm: bool = True):
+        """Greedy LDTW path cost per window in the reference's own FP32
+        arithmetic (ztsh2_ldtw, or tsh2_ldtw with znorm=False), float32."""
+        _dev(subject, torch.float32, "subject")
+        out = torch.empty(subject.numel() - self.M + 1, dtype=torch.float32, device=subject.device)
+        self._check(self._lib.ldtw_ref_all_windows(self._h, _ptr(subject), subject.numel(),
+                                                   _metric(metric), int(bool(znorm)), _ptr(out)))
+        return out
+
+    def ldtw_ref_search_host(self, query, subject, W, metric=EUCLIDEAN, znorm: bool = True):
+        """GPU-LDTW as the reference computes it (FP32): (location, distance)."""
+        q = np.ascontiguousarray(query, dtype=np.float32)
+        s = np.ascontiguousarray(subject, dtype=np.float32)
+        loc, dist = ctypes.c_int64(), ctypes.c_float()
+        self._check(self._lib.ldtw_ref_search_host(self._h, _ptr(q), q.size, _ptr(s), s.size, W,
+                                                   _metric(metric), int(bool(znorm)),
+                                                   ctypes.byref(loc), ctypes.byref(dist)))
         self.M, self.W = q.size, min(W, q.size - 1)
         return loc.value, dist.value
 

@@ -73,6 +73,7 @@ static int ensure_query_mem(cdtw_handle h, int M, int W) {
     const size_t o_zq64 = c.take<double>(M);
     const int lqr = qrev_len(M, W);
     const size_t o_qrev = c.take<float>(4 * (size_t)lqr);
+    const size_t o_qraw = c.take<float>(M);
     const size_t bytes = c.off;
     if (bytes > h->qmem_bytes) {
         CDTW_TRY(check_memory_limit(h, h->qmem_bytes, bytes, "query pack"));
@@ -96,6 +97,7 @@ static int ensure_query_mem(cdtw_handle h, int M, int W) {
     q.lqr = lqr;
     q.qrev_base = qrev_hi(M, W);
     q.qrev = (float*)(base + o_qrev);
+    q.qraw = (float*)(base + o_qraw);
     return CDTW_OK;
 }
 
@@ -174,6 +176,7 @@ int cdtw_destroy(cdtw_handle h) {
     cudaStreamSynchronize(h->stream);
     if (h->own_stream) cudaStreamSynchronize(h->own_stream);
     batch_plan_release(h);
+    stream_release(h);
     if (h->ws) cudaFree(h->ws);
     if (h->qmem) cudaFree(h->qmem);
     if (h->ring) cudaFree(h->ring);
@@ -581,6 +584,63 @@ int ldtw_search_host(cdtw_handle h, const float* h_query, int M, const float* h_
     CDTW_CUDA(h, cudaStreamSynchronize(h->stream));
     if (location) *location = pin->i;
     if (distance) *distance = metric == CDTW_EUCLIDEAN ? sqrt(pin->v) : pin->v;
+    return CDTW_OK;
+}
+
+int ldtw_ref_all_windows(cdtw_handle h, const float* d_subject, int64_t N, int metric, int znorm,
+                         float* d_out) {
+    if (!h) return CDTW_EINVAL;
+    if (!h->has_query) return set_error(h, CDTW_EINVAL, "no query set (cdtw_set_query)");
+    if (!d_subject || !d_out) return set_error(h, CDTW_EINVAL, "null pointer");
+    if (!valid_metric(metric)) return set_error(h, CDTW_EINVAL, "bad metric %d", metric);
+    const int M = h->q.M;
+    if (N < M) return set_error(h, CDTW_EINVAL, "subject shorter than query");
+    if (N - M + 1 > INT32_MAX) return set_error(h, CDTW_EUNSUPPORTED, "too many windows");
+    CDTW_CUDA(h, cudaSetDevice(h->device));
+    Carver c;
+    const size_t o_q = c.take<float>(M);
+    CDTW_TRY(ensure_workspace(h, c.off));
+    return launch_ldtw_ref(h, d_subject, N, metric == CDTW_EUCLIDEAN, znorm != 0,
+                           (float*)((char*)h->ws + o_q), d_out);
+}
+
+int ldtw_ref_search_host(cdtw_handle h, const float* h_query, int M, const float* h_subject,
+                         int64_t N, int W, int metric, int znorm, int64_t* location,
+                         float* distance) {
+    if (!h) return CDTW_EINVAL;
+    if (!h_query || !h_subject) return set_error(h, CDTW_EINVAL, "null pointer");
+    if (!valid_metric(metric)) return set_error(h, CDTW_EINVAL, "bad metric %d", metric);
+    if (M < 1 || N < M) return set_error(h, CDTW_EINVAL, "need 1 <= M <= N");
+    const int64_t Nw = N - M + 1;
+    if (Nw > INT32_MAX) return set_error(h, CDTW_EUNSUPPORTED, "too many windows");
+    CDTW_CUDA(h, cudaSetDevice(h->device));
+    Carver c;
+    const size_t o_x = c.take<float>(N);
+    const size_t o_q = c.take<float>(M);
+    const size_t o_d = c.take<float>(Nw);
+    const size_t o_k = c.take<unsigned long long>(1);
+    CDTW_TRY(ensure_workspace(h, c.off));
+    char* base = (char*)h->ws;
+    float* dx = (float*)(base + o_x);
+    CDTW_CUDA(h, cudaMemcpyAsync(dx, h_subject, sizeof(float) * N, cudaMemcpyHostToDevice,
+                                 h->stream));
+    CDTW_TRY(cdtw_set_query(h, h_query, M, W, CDTW_HOST));
+    CDTW_TRY(launch_ldtw_ref(h, dx, N, metric == CDTW_EUCLIDEAN, znorm != 0,
+                             (float*)(base + o_q), (float*)(base + o_d)));
+    unsigned long long* key = (unsigned long long*)(base + o_k);
+    CDTW_CUDA(h, cudaMemsetAsync(key, 0xff, sizeof(unsigned long long), h->stream));
+    CDTW_TRY(launch_argmin_f32(h, (float*)(base + o_d), Nw, key));
+    unsigned long long* pin = (unsigned long long*)h->pinned;
+    CDTW_CUDA(h, cudaMemcpyAsync(pin, key, sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                                 h->stream));
+    CDTW_CUDA(h, cudaStreamSynchronize(h->stream));
+    if (*pin == ~0ull)
+        return set_error(h, CDTW_EINVAL, "no window has a finite LDTW cost");
+    const uint32_t bits = (uint32_t)(*pin >> 32);
+    float d;
+    memcpy(&d, &bits, 4);
+    if (location) *location = (int64_t)(uint32_t)*pin;
+    if (distance) *distance = metric == CDTW_EUCLIDEAN ? sqrtf(d) : d;
     return CDTW_OK;
 }
 

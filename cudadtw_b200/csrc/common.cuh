@@ -41,6 +41,7 @@ struct QueryPack {
     int lqr = 0;           // floats per qrev copy (multiple of 4)
     int qrev_base = 0;     // A
     float* qrev = nullptr; // 4 * lqr floats
+    float* qraw = nullptr; // M floats: the query as given (optional)
 };
 
 // Extent of the reversed extended query for strips of up to kStripRowsMax rows.
@@ -63,6 +64,8 @@ struct cdtw_handle_s {
     size_t ws_bytes = 0;
     // cached plan of the batched search (batch_host.cu)
     void* batch = nullptr;
+    // state of an incremental search over a stream (stream.cu)
+    void* stream_state = nullptr;
     // boundary rings of the strip kernel's resident warps (grow-only)
     void* ring = nullptr;
     size_t ring_bytes = 0;
@@ -94,6 +97,7 @@ namespace cdtw {
 
 int set_error(cdtw_handle h, int status, const char* fmt, ...);
 void batch_plan_release(cdtw_handle h);
+void stream_release(cdtw_handle h);
 // top-k non-overlapping matches (search.cu)
 size_t topk_workspace_bytes(int64_t N, int M, int W);
 int run_topk(cdtw_handle h, const float* x, int64_t N, const double* mu, const float* sigma,
@@ -293,6 +297,13 @@ int launch_ed(cdtw_handle h, const double* x, int64_t N, const double* zq, int M
               const double* sigma, double* out);
 int launch_ldtw(cdtw_handle h, const float* x, int64_t N, const double* mu, const double* sigma,
                 bool euclid, double* out);
+// The reference's FP32 LDTW (ztsh2_ldtw / tsh2_ldtw arithmetic); qwork: M
+// floats of device scratch for the reference-normalised query.
+int launch_ldtw_ref(cdtw_handle h, const float* x, int64_t N, bool euclid, bool znorm,
+                    float* qwork, float* out);
+// Packed (float bits, index) minimum of out[0..n) into *key (first strict
+// minimum; NaN skipped); *key must start at ~0.
+int launch_argmin_f32(cdtw_handle h, const float* v, int64_t n, unsigned long long* key);
 int launch_prepare_query(cdtw_handle h, const float* d_query_raw, int M, int W);
 // One block per query: prepares packs[q] from the raw query at raw + offs[q].
 int launch_prepare_queries(cdtw_handle h, const float* raw, const int64_t* offs,
@@ -336,8 +347,11 @@ int launch_lb_keogh(cdtw_handle h, const float* x, int64_t N, const double* mu,
 int launch_cdtw_search(cdtw_handle h, const float* x, int64_t N, const double* mu,
                        const float* sigma, const Cand* cands, const int* count, int* work,
                        int max_count, bool euclid, unsigned long long* key);
-size_t search_workspace_bytes(int64_t N, int M, int W);
+// init_key: a device key the search starts from (a bound carried over from
+// earlier parts of a stream), else no bound.
 int run_search(cdtw_handle h, const float* x, int64_t N, const double* mu, const float* sigma,
-               bool euclid, char* ws_base, unsigned long long** key_out, int** ctr_out);
+               bool euclid, char* ws_base, unsigned long long** key_out, int** ctr_out,
+               const unsigned long long* init_key = nullptr);
+size_t search_workspace_bytes(int64_t N, int M, int W);
 
 }  // namespace cdtw

@@ -602,13 +602,19 @@ size_t search_workspace_bytes(int64_t N, int M, int W) {
 // Runs the whole pruned search; the result key and the stage counts stay on
 // the device (ws key / counters) for the caller to read.
 int run_search(cdtw_handle h, const float* x, int64_t N, const double* mu, const float* sigma,
-               bool euclid, char* ws_base, unsigned long long** key_out, int** ctr_out) {
+               bool euclid, char* ws_base, unsigned long long** key_out, int** ctr_out,
+               const unsigned long long* init_key) {
     const QueryPack& q = h->q;
     const int64_t Nw = N - q.M + 1;
     SearchWs ws;
     carve_search(N, Nw, q.M, q.W, &ws, ws_base);
     CDTW_CUDA(h, cudaMemsetAsync(ws.ctr, 0, sizeof(int) * 8, h->stream));
-    CDTW_CUDA(h, cudaMemsetAsync(ws.key, 0xff, sizeof(unsigned long long), h->stream));
+    if (init_key) {
+        CDTW_CUDA(h, cudaMemcpyAsync(ws.key, init_key, sizeof(unsigned long long),
+                                     cudaMemcpyDeviceToDevice, h->stream));
+    } else {
+        CDTW_CUDA(h, cudaMemsetAsync(ws.key, 0xff, sizeof(unsigned long long), h->stream));
+    }
     // 1. LB_Kim of every window + per-block seeds
     const int64_t nblk = div_up(Nw, kKimBlock);
     CDTW_TRY(launch_lb_kim(h, x, N, mu, sigma, nullptr, Nw, euclid, ws.lbkim, ws.seeds,

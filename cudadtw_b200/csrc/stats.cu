@@ -129,6 +129,8 @@ __device__ __forceinline__ void prepare_query_body(const float* __restrict__ qra
         zs[i] = v;
         s += v;
     }
+    __syncthreads();  // qraw may be p.zq (a host query staged there)
+    for (int i = t; p.qraw && i < M; i += blockDim.x) p.qraw[i] = (float)zs[i];
     s = warp_sum(s);
     if (lane == 0) red[0][wid] = s;
     __syncthreads();

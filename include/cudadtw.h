@@ -157,6 +157,27 @@ int cdtw_topk(cdtw_handle h, const float* d_subject, int64_t N, const double* d_
 int cdtw_search_host(cdtw_handle h, const float* h_query, int M, const float* h_subject,
                      int64_t N, int W, int metric, int64_t* location, float* distance);
 
+/* ---- search over a stream that arrives in pieces ------------------------------ */
+
+/* The pruned search of cdtw_search_host over a subject that is pushed in
+ * pieces of any size and never held whole on the device: the avg_std epochs
+ * (include/stats.cuh:115-142) and the EPOCH loop of UCR_DTW_BIN.cpp:579-707,
+ * which carries the last m-1 samples and the best-so-far from chunk to
+ * chunk.  Samples are staged in chunks of `chunk` samples (0: 2^23); each
+ * chunk's copy to the device overlaps the search of the previous one, and
+ * every chunk's search starts from the best distance of the chunks before it
+ * (kept on the device).  The query (host, M >= 11 floats, band W) stays in
+ * the handle until cdtw_stream_end; the handle must not run other searches
+ * in between.  Windows are numbered from the first sample pushed (64-bit);
+ * ties keep the earliest window, as UCR_DTW_BIN.cpp:682.  cdtw_stream_end
+ * returns the best window, its printed distance (as cdtw_prune_cdtw) and the
+ * number of samples scanned, and sets the stage counts and termination flag
+ * (cdtw_search_counts / cdtw_search_flag) summed over the chunks. */
+int cdtw_stream_begin(cdtw_handle h, const float* h_query, int M, int W, int metric,
+                      int64_t chunk);
+int cdtw_stream_push(cdtw_handle h, const float* h_samples, int64_t n);
+int cdtw_stream_end(cdtw_handle h, int64_t* location, float* distance, int64_t* scanned);
+
 /* Stage counts of the last search on this handle: counts[0] windows,
  * counts[1] windows below the best-so-far after LB_Kim, counts[2] windows
  * that reached the cDTW stage.  No reference counterpart (UCR prints the
@@ -221,6 +242,28 @@ int ldtw_all_windows(cdtw_handle h, const float* d_subject, int64_t N, int metri
  * path cost for the Euclidean cost. */
 int ldtw_search_host(cdtw_handle h, const float* h_query, int M, const float* h_subject,
                      int64_t N, int W, int metric, int64_t* location, double* distance);
+
+/* LDTW in the reference's own FP32 arithmetic, for drop-in index parity with
+ * its GPU-LDTW.  znorm != 0: ztsh2_ldtw (include/ldtw.cuh:294-391) -- the
+ * query z-normalised as GPU-ldtw.cu does on the host (znormalize,
+ * stats.cuh:8-28, float sums), window statistics as avg_std<double>
+ * (stats.cuh:30-52: FP64 window sums, variance E[x^2]-mu^2 in float),
+ * samples (s-avg)/std, costs, comparisons and the path sum in float.
+ * znorm == 0: tsh2_ldtw (ldtw.cuh:199-291) / serial_ldtw (:19-71), the query
+ * as given to cdtw_set_query against the raw windows.  d_out: N-M+1 float
+ * path costs (squared for CDTW_EUCLIDEAN).  Its decisions can differ from
+ * ldtw_all_windows' FP64 ones on near-ties; on level-shifted series the
+ * float variance loses precision exactly as the reference's does. */
+int ldtw_ref_all_windows(cdtw_handle h, const float* d_subject, int64_t N, int metric, int znorm,
+                         float* d_out);
+
+/* The whole GPU-LDTW search in the reference's arithmetic from host buffers
+ * (GPU-ldtw.cu:44-98 with ztsh2_ldtw, or its tsh2_ldtw line :87-88 when
+ * znorm == 0): first strict minimum (determine_min, ldtw.cuh:177-192);
+ * *distance = sqrt of the path cost for CDTW_EUCLIDEAN. */
+int ldtw_ref_search_host(cdtw_handle h, const float* h_query, int M, const float* h_subject,
+                         int64_t N, int W, int metric, int znorm, int64_t* location,
+                         float* distance);
 
 /* ---- fixed-scratch entry point ------------------------------------------------ */
 

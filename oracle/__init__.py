@@ -37,9 +37,9 @@ def build() -> None:
     binaries into _ref/ (kept when already built)."""
     subprocess.run(["make", "-s", "-C", HERE, "all"], check=True)
     refdir = os.environ.get("CDTW_REFERENCE_DIR", "")
-    if refdir and os.path.isdir(refdir) and not (
-            os.path.exists(os.path.join(REF_DIR, "UCR_DTW_BIN"))
-            and os.path.exists(os.path.join(REF_DIR, "UCR_ED_BIN"))):
+    if refdir and os.path.isdir(refdir) and not all(
+            os.path.exists(os.path.join(REF_DIR, b))
+            for b in ("UCR_DTW_BIN", "UCR_ED_BIN", "UCR_DTW", "ref_ldtw")):
         subprocess.run(["make", "-s", "-C", HERE, "ref", f"REFDIR={refdir}"], check=True)
 
 
@@ -301,6 +301,38 @@ class UcrShards:
         exact = cdtw_list(q, self.x, w, np.array(locs, dtype=np.int64))
         best = min(range(len(jobs)), key=lambda s: (exact[s], locs[s]))
         return locs[best], dists[best], wall, cpus
+
+
+def write_text(path: str, v: np.ndarray) -> None:
+    """One value per line, each float32 printed exactly (9 significant digits
+    round-trip), so a text reader recovers the float32 values."""
+    np.savetxt(path, np.asarray(v, np.float32).astype(np.float64), fmt="%.9g")
+
+
+def ucr_dtw_text(data_path: str, query_path: str, m: int, r_arg: str):
+    """Run the reference UCR_DTW (text input, UCR_DTW.cpp:381-427) on files.
+    Returns (location, distance, cpu_s, stdout)."""
+    return _run_ucr("UCR_DTW", [data_path, query_path, str(m), r_arg])
+
+
+def ref_ldtw(q: np.ndarray, x: np.ndarray, w: int, znorm: bool = True):
+    """The reference's own LDTW host code (z_serial_ldtw / serial_ldtw of
+    include/ldtw.cuh, built into _ref/ref_ldtw) on every window, with the
+    inputs its GPU-ldtw.cu makes (FP32 query z-normalisation, avg_std window
+    statistics).  Returns (float32 costs per window, determine_min's index)."""
+    path = os.path.join(REF_DIR, "ref_ldtw")
+    if not os.path.exists(path):
+        raise FileNotFoundError(f"{path} missing: run `make -C oracle ref`")
+    with tempfile.TemporaryDirectory() as d:
+        qp, xp, rp = (os.path.join(d, n) for n in ("q.bin", "s.bin", "r.bin"))
+        np.ascontiguousarray(q, np.float32).tofile(qp)
+        np.ascontiguousarray(x, np.float32).tofile(xp)
+        out = subprocess.run([path, qp, xp, str(q.size), str(x.size), str(w),
+                              "z" if znorm else "raw", rp], check=True, stdout=subprocess.PIPE,
+                             text=True).stdout
+        r = np.fromfile(rp, dtype=np.float32)
+    loc = int(re.search(r"found at index (\d+)", out).group(1))
+    return r, loc
 
 
 def ucr_ed(x: np.ndarray, q: np.ndarray):
