@@ -29,6 +29,8 @@ struct RegKernels {
     RegSearchKernel smh[kMaxRegW + 1];
     RegKernel eu2[kMaxReg2W + 1];  // two windows per thread
     RegKernel mh2[kMaxReg2W + 1];
+    RegKernel eu4[kMaxReg4W + 1];  // four windows per thread
+    RegKernel mh4[kMaxReg4W + 1];
     RegKernels() {
         void** a = (void**)eu;
         void** b = (void**)mh;
@@ -42,6 +44,7 @@ struct RegKernels {
         reg_fill_part5(a, b, c, d);
         reg2_fill_part0((void**)eu2, (void**)mh2);
         reg2_fill_part1((void**)eu2, (void**)mh2);
+        reg4_fill_part0((void**)eu4, (void**)mh4);
     }
 };
 
@@ -117,17 +120,19 @@ int launch_cdtw_windows(cdtw_handle h, const float* x, int64_t N, const double* 
                                  variant == CDTW_VARIANT_STRIP16 ? 16 : 32, out);
     }
     if (L <= 0) return CDTW_OK;
-    // two windows per thread up to W = kMaxReg2W (register budget)
-    const bool two = q.W <= kMaxReg2W;
-    RegKernel k = two ? (euclid ? reg_kernels().eu2[q.W] : reg_kernels().mh2[q.W])
-                      : (euclid ? reg_kernels().eu[q.W] : reg_kernels().mh[q.W]);
+    // four windows per thread up to W = kMaxReg4W, two up to kMaxReg2W
+    // (register budget)
+    const int per = q.W <= kMaxReg4W ? 4 : (q.W <= kMaxReg2W ? 2 : 1);
+    RegKernel k = per == 4   ? (euclid ? reg_kernels().eu4[q.W] : reg_kernels().mh4[q.W])
+                  : per == 2 ? (euclid ? reg_kernels().eu2[q.W] : reg_kernels().mh2[q.W])
+                             : (euclid ? reg_kernels().eu[q.W] : reg_kernels().mh[q.W]);
     const int lq4 = q.lq / 4;
     const size_t smem = (size_t)q.lq * 4 * sizeof(float);
     if (smem > 48 * 1024)
         CDTW_CUDA(h, cudaFuncSetAttribute((const void*)k,
                                           cudaFuncAttributeMaxDynamicSharedMemorySize,
                                           (int)smem));
-    const unsigned blocks = (unsigned)div_up(two ? div_up(L, 2) : L, kRegBlock);
+    const unsigned blocks = (unsigned)div_up(div_up(L, per), kRegBlock);
     k<<<blocks, kRegBlock, smem, h->stream>>>(x, mu, sigma, (const float4*)q.qpad, lq4, q.M, Nw,
                                               idx, (int)L, out);
     CDTW_LAUNCH(h, "cdtw_reg_kernel");

@@ -164,6 +164,88 @@ cdtw_reg2_kernel(const float* __restrict__ x, const double* __restrict__ mu,
     if (2 * t + 1 < L) out[2 * t + 1] = ok1 ? r1 : __int_as_float(0x7fc00000);
 }
 
+// Four windows per thread for narrow bands: the query band values of a row
+// are loaded once for 4(2W+1) cells and four independent min chains
+// interleave (listed windows 4t .. 4t+3; missing ones repeat the last listed
+// window and are not stored).
+constexpr int kMaxReg4W = 16;
+
+template <int W, bool EU>
+__global__ void __launch_bounds__(kRegBlock, 1)
+cdtw_reg4_kernel(const float* __restrict__ x, const double* __restrict__ mu,
+                 const float* __restrict__ sigma, const float4* __restrict__ qpad4, int lq4,
+                 int M, int Nw, const int32_t* __restrict__ idx, int L, float* __restrict__ out) {
+    extern __shared__ float4 sq4[];
+    for (int e = threadIdx.x; e < 4 * lq4; e += blockDim.x) sq4[e] = qpad4[e];
+    __syncthreads();
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (4 * t >= L) return;
+    constexpr int NW = 4;
+    constexpr int B = 2 * W + 1;
+    constexpr int NQ4 = (B + 3) / 4;
+    Norm nm[NW];
+    const float* xw[NW];
+    bool ok[NW];
+#pragma unroll
+    for (int v = 0; v < NW; ++v) {
+        const int tv = min(4 * t + v, L - 1);
+        int w = idx ? idx[tv] : tv;
+        ok[v] = w >= 0 && w < Nw;
+        if (!ok[v]) w = 0;  // a listed window outside the subject: NaN, no access
+        nm[v] = make_norm(mu[w], sigma[w]);
+        xw[v] = x + w;
+    }
+    float p[NW][B + 1];
+#pragma unroll
+    for (int v = 0; v < NW; ++v) {
+#pragma unroll
+        for (int k = 0; k <= B; ++k) p[v][k] = CDTW_INF;
+        p[v][W] = 0.0f;
+    }
+    float r[NW];
+#pragma unroll
+    for (int v = 0; v < NW; ++v) r[v] = CDTW_INF;
+    for (int j0 = 0; j0 < M; j0 += 4) {
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int j = j0 + u;
+            const int jc = min(j, M - 1);
+            float z[NW];
+#pragma unroll
+            for (int v = 0; v < NW; ++v) z[v] = znorm(nm[v], __ldg(xw[v] + jc));
+            const float4* qr = sq4 + u * lq4 + (j0 >> 2);
+            float qv[NQ4 * 4];
+#pragma unroll
+            for (int q4 = 0; q4 < NQ4; ++q4) {
+                const float4 a = qr[q4];
+                qv[4 * q4 + 0] = a.x;
+                qv[4 * q4 + 1] = a.y;
+                qv[4 * q4 + 2] = a.z;
+                qv[4 * q4 + 3] = a.w;
+            }
+            float l[NW];
+#pragma unroll
+            for (int v = 0; v < NW; ++v) l[v] = CDTW_INF;
+#pragma unroll
+            for (int k = 0; k < B; ++k) {
+#pragma unroll
+                for (int v = 0; v < NW; ++v) {
+                    const float m = min3f(p[v][k], p[v][k + 1], l[v]);
+                    l[v] = cell<EU>(z[v] - qv[k], m);
+                    p[v][k] = l[v];  // p[v][k] is not read again this row
+                }
+            }
+            if (j == M - 1) {
+#pragma unroll
+                for (int v = 0; v < NW; ++v) r[v] = p[v][W];
+            }
+        }
+    }
+#pragma unroll
+    for (int v = 0; v < NW; ++v)
+        if (4 * t + v < L) out[4 * t + v] = ok[v] ? r[v] : __int_as_float(0x7fc00000);
+}
+
 // cDTW of one window (xw, normalisation nm) against the query whose padded
 // copies sit in shared memory (sq4, lq4 float4 per copy) with its envelope
 // senv, abandoning once the last row minimum plus the remaining suffix of the
@@ -318,6 +400,17 @@ struct Reg2Range {
     }
 };
 
+template <int LO, int HI>
+struct Reg4Range {
+    static void fill(RegKernel* eu, RegKernel* mh) {
+        if constexpr (LO <= HI) {
+            eu[LO] = cdtw_reg4_kernel<LO, true>;
+            mh[LO] = cdtw_reg4_kernel<LO, false>;
+            Reg4Range<LO + 1, HI>::fill(eu, mh);
+        }
+    }
+};
+
 // Defined in cdtw_reg_part*.cu: each fills its range of bands.
 void reg_fill_part0(void** eu, void** mh, void** seu, void** smh);
 void reg_fill_part1(void** eu, void** mh, void** seu, void** smh);
@@ -327,5 +420,6 @@ void reg_fill_part4(void** eu, void** mh, void** seu, void** smh);
 void reg_fill_part5(void** eu, void** mh, void** seu, void** smh);
 void reg2_fill_part0(void** eu, void** mh);  // two-window kernels, cdtw_reg2_part*.cu
 void reg2_fill_part1(void** eu, void** mh);
+void reg4_fill_part0(void** eu, void** mh);  // four-window kernels, cdtw_reg4_part0.cu
 
 }  // namespace cdtw
