@@ -451,9 +451,12 @@ def subresults(h, dev) -> dict:
         D = torch.empty(n, device=dev)
         gq, gs = torch.empty_like(q), torch.empty_like(s)
         fns = {"fwd": lambda: h.pair_fwd(q, s, W, out=D),
-               "fwd_path": lambda: h.pair_fwd(q, s, W, path=path, out=D),
+               "fwd_path": lambda: h.pair_fwd(q, s, W, path=path, out=D, mode="store"),
+               "fwd_path_recompute": lambda: h.pair_fwd(q, s, W, path=path, out=D,
+                                                        mode="recompute"),
                "bwd": lambda: h.pair_bwd(q, s, path, dq=gq, ds=gs)}
         fns["fwd_bwd"] = lambda: (fns["fwd_path"](), fns["bwd"]())
+        fns["fwd_bwd_recompute"] = lambda: (fns["fwd_path_recompute"](), fns["bwd"]())
         r = {}
         side = torch.cuda.Stream(dev)
         h.use_torch_stream(side)
@@ -479,9 +482,12 @@ def subresults(h, dev) -> dict:
         c = cells(L, W)
         r["fwd_gcups"] = n * c / (r["fwd_ms"] / 1e3) / 1e9
         r["fwd_bwd_over_fwd"] = r["fwd_bwd_ms"] / r["fwd_ms"]
-        scratch = h.pair_workspace_bytes(1, L, W, False, True)
+        r["fwd_bwd_recompute_over_fwd"] = r["fwd_bwd_recompute_ms"] / r["fwd_ms"]
+        scratch = h.pair_workspace_bytes(1, L, W, False, True, mode="store")
         r["bytes_per_pair"] = {"path_record": h.pair_path_bytes(1, L),
                                "direction_scratch": scratch,
+                               "checkpoint_scratch": h.pair_workspace_bytes(
+                                   1, L, W, False, True, mode="recompute"),
                                "full_fp32_band_table": 4 * c}
         r["direction_record_in"] = "shared memory" if scratch == 0 else "device scratch"
         pair[f"{n}x{L}_W{W}"] = r

@@ -57,6 +57,7 @@ SIGNATURES = {
     "cdtw_refine_templates": (c_int, [c_vp, c_vp, c_i64, c_vp, c_vp, c_vp, c_int, c_vp, c_int,
                                       c_int, ctypes.c_float, c_int, c_vp]),
     "cdtw_pair_workspace_bytes": (ctypes.c_size_t, [c_i64, c_int, c_int, c_int, c_int]),
+    "cdtw_pair_last_mode": (c_int, [c_vp, ctypes.POINTER(c_int)]),
     "cdtw_pair_fwd": (c_int, [c_vp, c_vp, c_vp, c_i64, c_int, c_int, c_int, c_int, c_vp, c_vp]),
     "cdtw_pair_bwd": (c_int, [c_vp, c_vp, c_vp, c_i64, c_int, c_int, c_int, c_vp, c_vp, c_vp,
                               c_vp]),

@@ -344,27 +344,37 @@ class Handle:
         """Bytes of the path record cdtw_pair_fwd writes for n pairs of length L."""
         return int(self._lib.cdtw_pair_path_bytes(n, L))
 
+    PAIR_MODES = {None: 0, "auto": 0, "store": 2, "recompute": 4}
+
     def pair_workspace_bytes(self, n: int, L: int, W: int, znorm: bool = True,
-                             with_path: bool = True) -> int:
+                             with_path: bool = True, mode=None) -> int:
         """Device work memory pair_fwd takes from the handle's workspace."""
-        return int(self._lib.cdtw_pair_workspace_bytes(n, L, W, self.PAIR_ZNORM if znorm else 0,
-                                                       int(with_path)))
+        flags = (self.PAIR_ZNORM if znorm else 0) | self.PAIR_MODES[mode]
+        return int(self._lib.cdtw_pair_workspace_bytes(n, L, W, flags, int(with_path)))
+
+    def pair_last_mode(self) -> str:
+        """"recompute" or "store": how the last pair_fwd with a path recorded it."""
+        r = ctypes.c_int()
+        self._check(self._lib.cdtw_pair_last_mode(self._h, ctypes.byref(r)))
+        return "recompute" if r.value else "store"
 
     def pair_fwd(self, q: torch.Tensor, s: torch.Tensor, W: int, metric=EUCLIDEAN,
                  znorm: bool = True, path: torch.Tensor | None = None,
-                 out: torch.Tensor | None = None) -> torch.Tensor:
+                 out: torch.Tensor | None = None, mode=None) -> torch.Tensor:
         """Banded cDTW of every pair (q[p], s[p]) (device (n, L) float32).  With
         ``path`` (a uint8 device buffer of pair_path_bytes) the optimal path is
-        recorded for pair_bwd."""
+        recorded for pair_bwd; ``mode`` "store" (2-bit directions) or
+        "recompute" (checkpoints, segments recomputed during the walk), None
+        for the library's choice by memory."""
         _dev(q, torch.float32, "q")
         _dev(s, torch.float32, "s")
         if q.shape != s.shape or q.dim() != 2:
             raise ValueError("q and s must both be (n, L)")
         n, L = q.shape
         D = out if out is not None else torch.empty(n, dtype=torch.float32, device=q.device)
+        flags = (self.PAIR_ZNORM if znorm else 0) | self.PAIR_MODES[mode]
         self._check(self._lib.cdtw_pair_fwd(self._h, _ptr(q), _ptr(s), n, L, int(W),
-                                            _metric(metric), self.PAIR_ZNORM if znorm else 0,
-                                            _ptr(D), _ptr(path)))
+                                            _metric(metric), flags, _ptr(D), _ptr(path)))
         return D
 
     def pair_bwd(self, q: torch.Tensor, s: torch.Tensor, path: torch.Tensor, dD=None,

@@ -649,17 +649,43 @@ size_t cdtw_pair_path_bytes(int64_t n, int L) {
     return (size_t)n * 32 + (size_t)n * L * 8;
 }
 
+// Default cap on the direction scratch of one cdtw_pair_fwd call with a path
+// record; above it (or above half the handle's memory limit) the forward
+// recomputes from checkpoints instead.
+static const size_t kPairDirBudget = (size_t)4 << 30;
+
+// Path mode of a forward with a path record: true for the checkpointed
+// recomputation, false for the stored direction bits.
+static bool pair_recompute(size_t mem_limit, int64_t n, int L, int W, int flags) {
+    if (pair_ckpt_floats(L, W) == 0) return false;  // shared-record pairs: no choice
+    if (flags & CDTW_PAIR_RECOMPUTE) return true;
+    if (flags & CDTW_PAIR_STORE_DIRS) return false;
+    const size_t budget = mem_limit ? std::min(kPairDirBudget, mem_limit / 2) : kPairDirBudget;
+    return (size_t)n * pair_dirs_words(L, W) * 4 > budget;
+}
+
+// Slices of the forward's work area: z copies, then the direction scratch or
+// the checkpoints.
+static size_t pair_carve(int64_t n, int L, int W, int flags, bool with_path, bool recompute,
+                         size_t* o_zq, size_t* o_zs, size_t* o_path) {
+    Carver c;
+    const bool zn = flags & CDTW_PAIR_ZNORM;
+    *o_zq = zn ? c.take<float>((size_t)n * L) : 0;
+    *o_zs = zn ? c.take<float>((size_t)n * L) : 0;
+    *o_path = 0;
+    if (with_path)
+        *o_path = recompute ? c.take<float>((size_t)n * pair_ckpt_floats(L, W))
+                            : c.take<uint32_t>((size_t)n * pair_dirs_words(L, W));
+    return c.off;
+}
+
 size_t cdtw_pair_workspace_bytes(int64_t n, int L, int W, int flags, int with_path) {
     if (n <= 0 || L < 1 || L > CDTW_MAX_QUERY || W < 0) return 0;
     W = std::min(W, L - 1);
     if (W > CDTW_PAIR_MAX_BAND) return 0;
-    Carver c;
-    if (flags & CDTW_PAIR_ZNORM) {
-        c.take<float>((size_t)n * L);
-        c.take<float>((size_t)n * L);
-    }
-    if (with_path) c.take<uint32_t>((size_t)n * pair_dirs_words(L, W));
-    return c.off;
+    size_t a, b, c;
+    return pair_carve(n, L, W, flags, with_path != 0, with_path && pair_recompute(0, n, L, W, flags),
+                      &a, &b, &c);
 }
 
 static int pair_check(cdtw_handle h, const float* q, const float* s, int64_t n, int L,
@@ -667,7 +693,11 @@ static int pair_check(cdtw_handle h, const float* q, const float* s, int64_t n, 
     if (!q || !s || n < 0 || L < 1 || L > CDTW_MAX_QUERY)
         return set_error(h, CDTW_EINVAL, "bad pair arguments (n=%lld L=%d)", (long long)n, L);
     if (!valid_metric(metric)) return set_error(h, CDTW_EINVAL, "bad metric %d", metric);
-    if (flags & ~CDTW_PAIR_ZNORM) return set_error(h, CDTW_EINVAL, "bad flags %d", flags);
+    if (flags & ~(CDTW_PAIR_ZNORM | CDTW_PAIR_STORE_DIRS | CDTW_PAIR_RECOMPUTE))
+        return set_error(h, CDTW_EINVAL, "bad flags %d", flags);
+    if ((flags & CDTW_PAIR_STORE_DIRS) && (flags & CDTW_PAIR_RECOMPUTE))
+        return set_error(h, CDTW_EINVAL, "CDTW_PAIR_STORE_DIRS and CDTW_PAIR_RECOMPUTE exclude "
+                                         "each other");
     if (n > (int64_t)INT32_MAX * 4) return set_error(h, CDTW_EINVAL, "too many pairs");
     return CDTW_OK;
 }
@@ -684,11 +714,11 @@ int cdtw_pair_fwd(cdtw_handle h, const float* d_q, const float* d_s, int64_t n, 
     if (d_path && ((uintptr_t)d_path & 7))
         return set_error(h, CDTW_EINVAL, "path record must be 8-byte aligned");
     const bool zn = flags & CDTW_PAIR_ZNORM;
-    Carver c;
-    const size_t o_zq = zn ? c.take<float>((size_t)n * L) : 0;
-    const size_t o_zs = zn ? c.take<float>((size_t)n * L) : 0;
-    const size_t o_dirs = d_path ? c.take<uint32_t>((size_t)n * pair_dirs_words(L, W)) : 0;
-    CDTW_TRY(ensure_workspace(h, c.off));
+    const bool recompute = d_path && pair_recompute(h->mem_limit, n, L, W, flags);
+    size_t o_zq, o_zs, o_dirs;
+    CDTW_TRY(ensure_workspace(
+        h, pair_carve(n, L, W, flags, d_path != nullptr, recompute, &o_zq, &o_zs, &o_dirs)));
+    h->last_pair_recompute = recompute ? 1 : 0;
     char* ws = (char*)h->ws;
     double* hdr = (double*)d_path;
     uint32_t* rows = d_path ? (uint32_t*)((char*)d_path + (size_t)n * 32) : nullptr;
@@ -701,8 +731,17 @@ int cdtw_pair_fwd(cdtw_handle h, const float* d_q, const float* d_s, int64_t n, 
         zq = (const float*)(ws + o_zq);
         zs = (const float*)(ws + o_zs);
     }
+    if (recompute)
+        return launch_pair_fwd_ckpt(h, zq, zs, n, L, W, metric == CDTW_EUCLIDEAN, d_D,
+                                    (float*)(ws + o_dirs), rows, cols);
     return launch_pair_fwd(h, zq, zs, n, L, W, metric == CDTW_EUCLIDEAN, d_D,
                            d_path ? (uint32_t*)(ws + o_dirs) : nullptr, rows, cols);
+}
+
+int cdtw_pair_last_mode(cdtw_handle h, int* recompute) {
+    if (!h || !recompute) return CDTW_EINVAL;
+    *recompute = h->last_pair_recompute;
+    return CDTW_OK;
 }
 
 int cdtw_pair_bwd(cdtw_handle h, const float* d_q, const float* d_s, int64_t n, int L,

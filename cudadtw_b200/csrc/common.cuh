@@ -83,6 +83,8 @@ struct cdtw_handle_s {
     int64_t last_counts[4] = {0, 0, 0, 0};
     // the last search's best distance lies below the largest LB_Kim
     int last_flag = 0;
+    // the last cdtw_pair_fwd with a path record recomputed from checkpoints
+    int last_pair_recompute = 0;
     // cDTW kernel variant per band (0 = built-in rule); set by the autotuner
     unsigned char band_variant[CDTW_MAX_QUERY] = {0};
     // host-buffer pipeline (cdtw_all_windows_host): copy-in, copy-out and a
@@ -114,6 +116,12 @@ int launch_pair_znorm(cdtw_handle h, const float* q, const float* s, int64_t n, 
 int launch_pair_fwd(cdtw_handle h, const float* zq, const float* zs, int64_t n, int L, int W,
                     bool euclid, float* D, uint32_t* dirs, uint32_t* rows, uint32_t* cols,
                     int64_t qstride = -1, const int* gate = nullptr, int gate_max = 0);
+// Checkpointed path record (memory: pair_ckpt_floats per pair instead of the
+// direction scratch); pair_ckpt_floats is 0 where the mode does not apply.
+size_t pair_ckpt_floats(int L, int W);
+int launch_pair_fwd_ckpt(cdtw_handle h, const float* zq, const float* zs, int64_t n, int L,
+                         int W, bool euclid, float* D, float* ckpt, uint32_t* rows,
+                         uint32_t* cols);
 int launch_pair_bwd(cdtw_handle h, const float* q, const float* s, int64_t n, int L,
                     const double* hdr, const uint32_t* rows, const uint32_t* cols,
                     const float* dD, bool euclid, float* dq, float* ds);

@@ -23,6 +23,7 @@
 // Jacobian (I - 11'/L - zz'/L) / sigma.
 #include "common.cuh"
 
+#include <algorithm>
 #include <type_traits>
 #include <utility>
 
@@ -48,6 +49,9 @@ struct PairArgs {
     int gate_max;         // the launch does nothing when it exceeds gate_max
     uint32_t* rows;       // per pair L words: a_i | b_i << 16
     uint32_t* cols;       // per pair L words: c_j | d_j << 16
+    float* ckpt;          // checkpointed mode: per pair nseg x 2C x G floats
+    int seg;              // anti-diagonals per segment (a multiple of 2C)
+    int nseg;             // segments per pair
 };
 
 // z-value of one sample with the pair header's mean and sigma (shared by the
@@ -121,7 +125,7 @@ struct PairLane {
 template <int C, int DM>
 __device__ __forceinline__ void store_dirs(const PairLane<C>& st, uint32_t* drow, int G, int l,
                                            int k, bool live) {
-    if constexpr (DM != 0) {
+    if constexpr (DM == 1 || DM == 2) {
         if (DM == 2 || live) ((DirT<C>*)drow)[(size_t)k * G + l] = (DirT<C>)st.bits;
     }
 }
@@ -171,7 +175,7 @@ __device__ __forceinline__ void body(PairLane<C>& st, const float* sq, const flo
                                      uint32_t* drow, int L, int G, int l, int& k, int K,
                                      bool live) {
     if constexpr (R < C) {
-        constexpr bool DIRS = DM != 0;
+        constexpr bool DIRS = DM == 1 || DM == 2;
         if (CHK && k >= K) return;
         step_odd<C, EU, DIRS, R, R + 1>(st, ss, L, G, l, true);
         store_dirs<C, DM>(st, drow, G, l, k, live);
@@ -371,11 +375,109 @@ __device__ __forceinline__ void walk_ring(const PairArgs& a, unsigned char* smem
     cp_async_wait<0>();
 }
 
+// Lane state at anti-diagonal 0 (D[-1][-1] = 0 under d = 0) and the first
+// one or two steps, up to the first step of parity 1 (k0 = 1 or 2), where the
+// bodies of 2C steps begin.  Returns k0.
+template <int C, bool EU, int DM>
+__device__ __forceinline__ int pair_begin(PairLane<C>& st, const float* sq, const float* ss,
+                                          uint32_t* drow, int L, int W, int G, int l, int K,
+                                          bool live) {
+    constexpr bool DIRS = DM == 1 || DM == 2;
+    const int e0 = W & 1;
+    const int p0 = l * C;
+    const int porg = W >> 1;  // slot of d = 0 on every anti-diagonal of parity e0
+#pragma unroll
+    for (int c = 0; c < C; ++c) {
+        const int p = p0 + c;
+        st.lim[c] = (p == W) ? CDTW_INF : -CDTW_INF;
+        const float org = (p == porg) ? 0.f : CDTW_INF;  // D[-1][-1] = 0 at k = -2
+        st.A[c] = e0 == 0 ? org : CDTW_INF;
+        st.B[c] = e0 == 0 ? CDTW_INF : org;
+        const int d = -W + 2 * p + e0;
+        const int i = -d / 2, j = d / 2;  // k = 0
+        st.Q[c] = (i >= 0 && i < L) ? __ldg(sq + i) : 0.f;
+        st.Sv[c] = (j >= 0 && j < L) ? __ldg(ss + j) : 0.f;
+    }
+    st.bits = 0;
+    st.iq = (W - e0) / 2;                      // lane 0's slot-0 query index at k = 0
+    st.js = (-W + 2 * (G * C - 1) + e0) / 2;  // lane G-1's last-slot subject index
+    st.pq = (st.iq + 1 < L) ? __ldg(sq + st.iq + 1) : 0.f;
+    st.ps = (st.js + 1 < L) ? __ldg(ss + st.js + 1) : 0.f;
+    int k = 0;
+    if (e0 == 0) {
+        step_even<C, EU, DIRS, 0, 0>(st, sq, L, G, l, false);
+        store_dirs<C, DM>(st, drow, G, l, k, live);
+        k = 1;
+    } else {
+        step_odd<C, EU, DIRS, 0, 0>(st, ss, L, G, l, false);
+        store_dirs<C, DM>(st, drow, G, l, k, live);
+        k = 1;
+        if (k < K) {
+            // query shift with the rotation kept at 0: move the window down
+            const float v = __shfl_up_sync(kFull, st.Q[C - 1], 1, G);
+#pragma unroll
+            for (int c = C - 1; c > 0; --c) st.Q[c] = st.Q[c - 1];
+            st.Q[0] = (l == 0) ? st.pq : v;
+            if (l == 0) {
+                ++st.iq;
+                st.pq = st.iq + 1 < L ? __ldg(sq + st.iq + 1) : 0.f;
+            }
+            step_even<C, EU, DIRS, 0, 0>(st, sq, L, G, l, false);
+            store_dirs<C, DM>(st, drow, G, l, k, live);
+            k = 2;
+        }
+    }
+    return k;
+}
+
+// Checkpoint s of a pair: the lane's two newest anti-diagonals at the start
+// of a body (A = k-1, B = k-2), slot-major so a group's lanes write adjacent
+// words.
+template <int C>
+__device__ __forceinline__ void ckpt_store(const PairLane<C>& st, float* ck, int G, int l,
+                                           bool live) {
+    if (!live) return;
+#pragma unroll
+    for (int c = 0; c < C; ++c) {
+        ck[(size_t)c * G + l] = st.A[c];
+        ck[(size_t)(C + c) * G + l] = st.B[c];
+    }
+}
+
+// Lane state at the start of the body whose first step is k (parity 1),
+// from checkpoint ck: the DP values, and the query / subject windows of step
+// k-1 (rotation 0) rebuilt from the series -- the values the forward held
+// there, so the recomputation is bit-identical.
+template <int C>
+__device__ __forceinline__ void ckpt_restore(PairLane<C>& st, const float* ck, const float* sq,
+                                             const float* ss, int L, int W, int G, int l, int k) {
+    const int p0 = l * C;
+    const int km = k - 1;                 // last anti-diagonal computed (parity 0)
+    const int em = (km + W) & 1;          // = 0
+#pragma unroll
+    for (int c = 0; c < C; ++c) {
+        const int p = p0 + c;
+        st.lim[c] = (p == W) ? CDTW_INF : -CDTW_INF;
+        st.A[c] = ck[(size_t)c * G + l];
+        st.B[c] = ck[(size_t)(C + c) * G + l];
+        const int d = -W + 2 * p + em;
+        const int i = (km - d) / 2, j = (km + d) / 2;
+        st.Q[c] = (i >= 0 && i < L) ? __ldg(sq + i) : 0.f;
+        st.Sv[c] = (j >= 0 && j < L) ? __ldg(ss + j) : 0.f;
+    }
+    st.bits = 0;
+    st.iq = (km + W - em) / 2;                            // lane 0, slot 0 at k-1
+    st.js = (km - W + 2 * (G * C - 1) + em) / 2;          // lane G-1, last slot at k-1
+    st.pq = (st.iq + 1 < L) ? __ldg(sq + st.iq + 1) : 0.f;
+    st.ps = (st.js + 1 < L) ? __ldg(ss + st.js + 1) : 0.f;
+}
+
 // DM: 0 distance only; 1 path record in global scratch, walked through a
-// shared-memory ring; 2 path record in shared memory (short pairs, C <= 4).
+// shared-memory ring; 2 path record in shared memory (short pairs, C <= 4);
+// 3 distance plus checkpoints every a.seg anti-diagonals (the path is then
+// recovered by pair_ckpt_walk_kernel).
 template <int C, bool EU, int DM>
 __global__ void __launch_bounds__(kPairThreads, 4) pair_fwd_kernel(const PairArgs a) {
-    constexpr bool DIRS = DM != 0;
     extern __shared__ __align__(16) unsigned char smem[];
     int64_t np = a.n;  // pairs present
     if (a.gate) {
@@ -401,53 +503,26 @@ __global__ void __launch_bounds__(kPairThreads, 4) pair_fwd_kernel(const PairArg
     const int p0 = l * C;
     const int porg = W >> 1;  // slot of d = 0 on every anti-diagonal of parity e0
     PairLane<C> st;
-#pragma unroll
-    for (int c = 0; c < C; ++c) {
-        const int p = p0 + c;
-        st.lim[c] = (p == W) ? CDTW_INF : -CDTW_INF;
-        const float org = (p == porg) ? 0.f : CDTW_INF;  // D[-1][-1] = 0 at k = -2
-        st.A[c] = e0 == 0 ? org : CDTW_INF;
-        st.B[c] = e0 == 0 ? CDTW_INF : org;
-        const int d = -W + 2 * p + e0;
-        const int i = -d / 2, j = d / 2;  // k = 0
-        st.Q[c] = (i >= 0 && i < L) ? __ldg(sq + i) : 0.f;
-        st.Sv[c] = (j >= 0 && j < L) ? __ldg(ss + j) : 0.f;
-    }
-    st.bits = 0;
-    st.iq = (W - e0) / 2;                      // lane 0's slot-0 query index at k = 0
-    st.js = (-W + 2 * (G * C - 1) + e0) / 2;  // lane G-1's last-slot subject index
-    st.pq = (st.iq + 1 < L) ? __ldg(sq + st.iq + 1) : 0.f;
-    st.ps = (st.js + 1 < L) ? __ldg(ss + st.js + 1) : 0.f;
     uint32_t* drow = DM == 1   ? a.dirs + (size_t)pr * a.dstride
                      : DM == 2 ? (uint32_t*)(smem + (size_t)gib * a.recb)
                                : nullptr;
-
-    int k = 0;
-    if (e0 == 0) {
-        step_even<C, EU, DIRS, 0, 0>(st, sq, L, G, l, false);
-        store_dirs<C, DM>(st, drow, G, l, k, live);
-        k = 1;
-    } else {
-        step_odd<C, EU, DIRS, 0, 0>(st, ss, L, G, l, false);
-        store_dirs<C, DM>(st, drow, G, l, k, live);
-        k = 1;
-        if (k < K) {
-            // query shift with the rotation kept at 0: move the window down
-            const float v = __shfl_up_sync(kFull, st.Q[C - 1], 1, G);
-#pragma unroll
-            for (int c = C - 1; c > 0; --c) st.Q[c] = st.Q[c - 1];
-            st.Q[0] = (l == 0) ? st.pq : v;
-            if (l == 0) {
-                ++st.iq;
-                st.pq = st.iq + 1 < L ? __ldg(sq + st.iq + 1) : 0.f;
-            }
-            step_even<C, EU, DIRS, 0, 0>(st, sq, L, G, l, false);
-            store_dirs<C, DM>(st, drow, G, l, k, live);
-            k = 2;
+    int k = pair_begin<C, EU, DM>(st, sq, ss, drow, L, W, G, l, K, live);
+    const int k0 = k;
+    float* ck = DM == 3 ? a.ckpt + (size_t)pr * a.nseg * 2 * C * G : nullptr;
+    while (k + 2 * C <= K) {
+        if constexpr (DM == 3) {
+            if (k > k0 && (k - k0) % a.seg == 0)
+                ckpt_store<C>(st, ck + (size_t)((k - k0) / a.seg) * 2 * C * G, G, l, live);
         }
+        body<C, EU, DM, false, 0>(st, sq, ss, drow, L, G, l, k, K, live);
     }
-    while (k + 2 * C <= K) body<C, EU, DM, false, 0>(st, sq, ss, drow, L, G, l, k, K, live);
-    if (k < K) body<C, EU, DM, true, 0>(st, sq, ss, drow, L, G, l, k, K, live);
+    if (k < K) {
+        if constexpr (DM == 3) {
+            if (k > k0 && (k - k0) % a.seg == 0)
+                ckpt_store<C>(st, ck + (size_t)((k - k0) / a.seg) * 2 * C * G, G, l, live);
+        }
+        body<C, EU, DM, true, 0>(st, sq, ss, drow, L, G, l, k, K, live);
+    }
 
     // D[L-1][L-1]: slot porg of the last anti-diagonal (parity e0)
     float dval = CDTW_INF;
@@ -459,6 +534,77 @@ __global__ void __launch_bounds__(kPairThreads, 4) pair_fwd_kernel(const PairArg
         walk_ring<C>(a, smem, drow, pr, L, K, G, l, gib, e0, porg, live);
     } else if constexpr (DM == 2) {
         walk_shared<C>(a, smem, drow, pr, L, K, G, l, gib, e0, porg, live);
+    }
+}
+
+// Path recovery of the checkpointed mode: per pair, the segments of a.seg
+// anti-diagonals from the last to the first are recomputed from their
+// checkpoints (segment 0 from the start) with direction bits into shared
+// memory, and lane 0 of the group walks the path back through each segment
+// as walk_ring does through its chunks; the group turns each segment's moves
+// into row and column runs.  Shared memory per group: a.recb bytes of
+// directions (seg x G elements) and a.logb bytes of move log (>= seg).
+template <int C, bool EU>
+__global__ void __launch_bounds__(kPairThreads, 4) pair_ckpt_walk_kernel(const PairArgs a) {
+    using DT = DirT<C>;
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int64_t np = a.n;
+    const int G = a.G, L = a.L, W = a.W;
+    const int tid = threadIdx.x;
+    const int l = tid & (G - 1);
+    const int gib = tid >> a.lgG;
+    const int64_t grp = (int64_t)blockIdx.x * (blockDim.x >> a.lgG) + gib;
+    if ((int64_t)blockIdx.x * (blockDim.x >> a.lgG) + ((tid & ~31) >> a.lgG) >= np) return;
+    const bool live = grp < np;
+    const int64_t pr = live ? grp : np - 1;
+    const float* sq = a.zq + pr * a.qstride;
+    const float* ss = a.zs + pr * L;
+    const int K = 2 * L - 1;
+    const int e0 = W & 1;
+    const int porg = W >> 1;
+    const int k0 = (e0 == 0) ? 1 : 2;
+    const float* ck = a.ckpt + (size_t)pr * a.nseg * 2 * C * G;
+    DT* rec = (DT*)(smem + (size_t)gib * a.recb);
+    uint8_t* mlog = smem + (size_t)(blockDim.x >> a.lgG) * a.recb + (size_t)gib * a.logb;
+    uint16_t* r16 = (uint16_t*)(a.rows + pr * L);  // [2i] = a_i, [2i+1] = b_i
+    uint16_t* c16 = (uint16_t*)(a.cols + pr * L);  // [2j] = c_j, [2j+1] = d_j
+    if (l == 0 && live) {
+        r16[2 * (L - 1) + 1] = (uint16_t)(L - 1);
+        c16[2 * (L - 1) + 1] = (uint16_t)(L - 1);
+    }
+    int kw = K - 1, e = e0;                // walker: anti-diagonal and its parity
+    int lw = porg / C, c = porg - lw * C;  // slot c of lane lw
+    int gi = L - 1, gj = L - 1;            // cell before the segment's first move
+    for (int s = a.nseg - 1; s >= 0; --s) {
+        const int kA = s == 0 ? 0 : k0 + s * a.seg;
+        const int kB = min(k0 + (s + 1) * a.seg, K);
+        // the record holds rows kA .. kB-1: store index k maps to row k - kA
+        uint32_t* drow = (uint32_t*)((char*)rec - (ptrdiff_t)kA * G * (ptrdiff_t)sizeof(DT));
+        PairLane<C> st;
+        int k;
+        if (s == 0) {
+            k = pair_begin<C, EU, 2>(st, sq, ss, drow, L, W, G, l, K, live);
+        } else {
+            ckpt_restore<C>(st, ck + (size_t)s * 2 * C * G, sq, ss, L, W, G, l, kA);
+            k = kA;
+        }
+        while (k + 2 * C <= kB) body<C, EU, 2, false, 0>(st, sq, ss, drow, L, G, l, k, kB, live);
+        if (k < kB) body<C, EU, 2, true, 0>(st, sq, ss, drow, L, G, l, k, kB, live);
+        __syncwarp();  // the segment's directions are visible to the walker
+        int nm = 0;
+        if (l == 0 && live) {
+            // every move lowers kw: at most kB - kA (<= a.logb) moves here
+            while (kw >= kA && (unsigned)lw < (unsigned)G) {
+                const uint32_t b = ((uint32_t)rec[(size_t)(kw - kA) * G + lw] >> (2 * c)) & 3u;
+                mlog[nm++] = (uint8_t)b;
+                walk_move<C>(b, kw, e, lw, c);
+            }
+        }
+        nm = __shfl_sync(kFull, nm, 0, G);
+        const int nmax = __reduce_max_sync(kFull, (unsigned)nm);
+        __syncwarp();
+        runs_from_moves<4>(mlog, nm, nmax, G, l, live, L, r16, c16, gi, gj);
+        __syncwarp();  // the record and the log are rewritten by the next segment
     }
 }
 
@@ -680,11 +826,17 @@ pair_bwd_kernel(const float* __restrict__ q, const float* __restrict__ s, int64_
 using PairFwdK = void (*)(const PairArgs);
 
 // dm 2 (shared record) is instantiated for C <= 4 only: the host selects it
-// for records of at most 512 bytes per lane, which needs C <= 4.
+// for records of at most 512 bytes per lane, which needs C <= 4.  dm 3 (the
+// checkpointed forward) and dm 4 (its path recovery) for C >= 2: the host
+// selects them only for pairs outside shared-record mode.
 template <int C>
 PairFwdK pick_fwd(bool eu, int dm) {
     if constexpr (C <= 4) {
         if (dm == 2) return eu ? pair_fwd_kernel<C, true, 2> : pair_fwd_kernel<C, false, 2>;
+    }
+    if constexpr (C >= 2) {
+        if (dm == 3) return eu ? pair_fwd_kernel<C, true, 3> : pair_fwd_kernel<C, false, 3>;
+        if (dm == 4) return eu ? pair_ckpt_walk_kernel<C, true> : pair_ckpt_walk_kernel<C, false>;
     }
     if (eu) return dm ? pair_fwd_kernel<C, true, 1> : pair_fwd_kernel<C, true, 0>;
     return dm ? pair_fwd_kernel<C, false, 1> : pair_fwd_kernel<C, false, 0>;
@@ -750,6 +902,27 @@ size_t pair_dirs_words(int L, int W) {
     return (size_t)(nch * kWalkChunk * G / 4);
 }
 
+// Checkpointed mode: anti-diagonals per segment (a multiple of 2C, about
+// 128) and segments per pair (segment 0 also covers the first one or two
+// steps before the bodies).
+static int pair_ckpt_seg(int C) { return 2 * C * std::max(2, 128 / (2 * C)); }
+
+static int pair_ckpt_nseg(int L, int W, int C) {
+    const int K = 2 * L - 1, k0 = (W & 1) ? 2 : 1;
+    return (int)std::max<int64_t>(1, div_up(std::max(K - k0, 1), pair_ckpt_seg(C)));
+}
+
+// Floats of checkpoints per pair in device scratch (two anti-diagonals of
+// G x C slots per segment); 0 where the pair runs in shared-record mode.
+size_t pair_ckpt_floats(int L, int W) {
+    int G, C;
+    pair_shape(L, W, &G, &C);
+    int recb, logb;
+    size_t shared_bytes;
+    if (C < 2 || pair_shared_record(L, G, C, &recb, &logb, &shared_bytes)) return 0;
+    return (size_t)pair_ckpt_nseg(L, W, C) * 2 * C * G;
+}
+
 int launch_pair_znorm(cdtw_handle h, const float* q, const float* s, int64_t n, int L, float* zq,
                       float* zs, double* hdr) {
     const int64_t warps = 2 * n;
@@ -782,6 +955,9 @@ int launch_pair_fwd(cdtw_handle h, const float* zq, const float* zs, int64_t n, 
     a.dstride = (int)pair_dirs_words(L, W);
     a.rows = rows;
     a.cols = cols;
+    a.ckpt = nullptr;
+    a.seg = 0;
+    a.nseg = 0;
     const int threads = kPairThreads;
     const int64_t groups_per_block = threads / G;
     // a path is recorded when the run arrays are given; the direction scratch
@@ -804,6 +980,57 @@ int launch_pair_fwd(cdtw_handle h, const float* zq, const float* zs, int64_t n, 
                                       (int)smem));
     k<<<(int)blocks, threads, smem, h->stream>>>(a);
     CDTW_LAUNCH(h, "pair_fwd_kernel");
+    return CDTW_OK;
+}
+
+// Checkpointed path record: the forward without direction bits storing
+// checkpoints every pair_ckpt_seg anti-diagonals, then the segment-wise
+// recomputation and walk (pair_ckpt_walk_kernel) writing the row and column
+// runs.  Needs C >= 2 outside shared-record mode (pair_ckpt_floats > 0).
+int launch_pair_fwd_ckpt(cdtw_handle h, const float* zq, const float* zs, int64_t n, int L,
+                         int W, bool euclid, float* D, float* ckpt, uint32_t* rows,
+                         uint32_t* cols) {
+    if (pair_ckpt_floats(L, W) == 0)
+        return set_error(h, CDTW_EUNSUPPORTED, "no checkpointed mode for L=%d W=%d", L, W);
+    int G, C;
+    pair_shape(L, W, &G, &C);
+    PairArgs a;
+    a.zq = zq;
+    a.zs = zs;
+    a.qstride = L;
+    a.gate = nullptr;
+    a.gate_max = 0;
+    a.n = n;
+    a.L = L;
+    a.W = W;
+    a.G = G;
+    a.lgG = 0;
+    while ((1 << a.lgG) < G) ++a.lgG;
+    a.D = D;
+    a.dirs = nullptr;
+    a.dstride = 0;
+    a.rows = rows;
+    a.cols = cols;
+    a.ckpt = ckpt;
+    a.seg = pair_ckpt_seg(C);
+    a.nseg = pair_ckpt_nseg(L, W, C);
+    const int threads = kPairThreads;
+    const int64_t groups_per_block = threads / G;
+    const int64_t blocks = div_up(n, groups_per_block);
+    if (blocks > INT32_MAX) return set_error(h, CDTW_EINVAL, "too many pairs");
+    const int eb = C <= 4 ? 1 : (C <= 8 ? 2 : 4);
+    // records of the longest segment (segment 0 holds up to seg + 2 rows)
+    a.recb = (int)round_up((int64_t)(a.seg + 2) * G * eb, 128) + 32;
+    a.logb = (int)round_up(a.seg + 2, 128) + 32;
+    const PairFwdK kf = fwd_kernel(C, euclid, 3);
+    kf<<<(int)blocks, threads, 0, h->stream>>>(a);
+    CDTW_LAUNCH(h, "pair_fwd_kernel");
+    const PairFwdK kw = fwd_kernel(C, euclid, 4);
+    const size_t smem = (size_t)groups_per_block * (size_t)(a.recb + a.logb);
+    CDTW_CUDA(h, cudaFuncSetAttribute((const void*)kw, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)smem));
+    kw<<<(int)blocks, threads, smem, h->stream>>>(a);
+    CDTW_LAUNCH(h, "pair_ckpt_walk_kernel");
     return CDTW_OK;
 }
 

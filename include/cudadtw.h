@@ -307,6 +307,8 @@ int cdtw_all_windows_noalloc(const float* d_query, int M, const float* d_subject
 /* ---- differentiable pairwise cDTW --------------------------------------------- */
 
 #define CDTW_PAIR_ZNORM 1      /* z-normalise both series of every pair */
+#define CDTW_PAIR_STORE_DIRS 2 /* path record from stored 2-bit directions */
+#define CDTW_PAIR_RECOMPUTE 4  /* path record recomputed from checkpoints */
 #define CDTW_PAIR_MAX_BAND 511 /* largest band W (after clamping W to L-1) */
 
 /* Bytes of the path record of n pairs of length L: per pair the
@@ -316,9 +318,28 @@ size_t cdtw_pair_path_bytes(int64_t n, int L);
 
 /* Device work memory cdtw_pair_fwd takes from the handle's grow-only workspace
  * for n pairs: z-normalised copies of both series (flags & CDTW_PAIR_ZNORM)
- * and, when a path is recorded (with_path != 0), 2 bits per band cell of
- * predecessor choices, padded to the lane layout.  0 for invalid sizes. */
+ * and, when a path is recorded (with_path != 0), either 2 bits per band cell
+ * of predecessor choices, padded to the lane layout, or (recomputation) two
+ * anti-diagonals of the band every ~128 anti-diagonals.  The mode is that of
+ * cdtw_pair_fwd without a memory limit on the handle.  0 for invalid sizes. */
 size_t cdtw_pair_workspace_bytes(int64_t n, int L, int W, int flags, int with_path);
+
+/* Path record modes of cdtw_pair_fwd (pairs whose record fits shared memory,
+ * 2L-1 <= 512 and band W <= 15, always keep it there).  Stored directions:
+ * the forward writes 2 bits per band cell to device scratch and walks them
+ * back.  Recomputation from checkpoints: the forward keeps only two
+ * anti-diagonals every ~128 (about 4x less scratch at L = 2048, W = 409),
+ * and the walk recomputes each segment, last first, with its direction bits
+ * in shared memory: the same path, bit for bit, for a second pass over the
+ * band.  CDTW_PAIR_STORE_DIRS / CDTW_PAIR_RECOMPUTE force a mode; without
+ * either, directions are stored unless their scratch would exceed 4 GiB (or
+ * half the handle's memory limit).  No reference counterpart (the DP of
+ * include/cdtw.cuh:24-88 returns distances only). */
+
+/* 1 when the last cdtw_pair_fwd with a path record on this handle recomputed
+ * from checkpoints, 0 when it stored direction bits.  No reference
+ * counterpart. */
+int cdtw_pair_last_mode(cdtw_handle h, int* recompute);
 
 /* Banded cDTW of n pairs (d_q[p], d_s[p]), each L float32 samples, row-major
  * n x L on the device: d_D[p] = minimum over warping paths with |i-j| <= W of

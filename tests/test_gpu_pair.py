@@ -112,6 +112,35 @@ def test_pair_full_workload_properties(handle):
     _check_fp64(q[idx], s[idx], W, True, D[idx], gq[idx], gs[idx], rows[idx], cols[idx])
 
 
+@pytest.mark.parametrize("L,W,n", [(300, 70, 40), (513, 130, 24), (1024, 204, 16),
+                                   (2048, 409, 8), (1100, 511, 6), (700, 9, 33)])
+@pytest.mark.parametrize("euclid", [True, False])
+def test_pair_recompute_equals_stored_directions(handle, L, W, n, euclid):
+    """The checkpointed mode recomputes each segment of anti-diagonals from
+    its checkpoint with the forward's own arithmetic, so its path record is
+    byte-identical to the stored-direction mode's, and so are D and the
+    gradients; checked against FP64 as well."""
+    rng = np.random.default_rng(L + 3 * W)
+    q, s = _walks(rng, n, L), _walks(rng, n, L)
+    dq_, ds_ = torch.from_numpy(q).cuda(), torch.from_numpy(s).cuda()
+    metric = 0 if euclid else 1
+    out = {}
+    for mode in ("store", "recompute"):
+        path = torch.empty(handle.pair_path_bytes(n, L), dtype=torch.uint8, device="cuda")
+        D = handle.pair_fwd(dq_, ds_, W, metric=metric, path=path, mode=mode)
+        assert handle.pair_last_mode() == mode
+        gq, gs = handle.pair_bwd(dq_, ds_, path, metric=metric)
+        out[mode] = (D.cpu().numpy(), path.cpu().numpy(), gq.cpu().numpy(), gs.cpu().numpy())
+    for a, b in zip(out["store"], out["recompute"]):
+        np.testing.assert_array_equal(a, b)
+    assert (handle.pair_workspace_bytes(n, L, W, mode="recompute") <
+            handle.pair_workspace_bytes(n, L, W, mode="store"))
+    D, raw, gq, gs = out["recompute"]
+    rows = raw[32 * n:32 * n + 4 * n * L].view(np.uint32).reshape(n, L)
+    cols = raw[32 * n + 4 * n * L:32 * n + 8 * n * L].view(np.uint32).reshape(n, L)
+    _check_fp64(q, s, W, euclid, D, gq, gs, rows, cols)
+
+
 def test_pair_forward_only_and_one_sided_backward(handle):
     rng = np.random.default_rng(5)
     n, L, W = 33, 200, 20
@@ -138,4 +167,7 @@ def test_pair_errors(handle):
         handle.pair_fwd(big, big, 10)
     with pytest.raises(CudaDTWError):
         handle._check(handle._lib.cdtw_pair_fwd(handle._h, q.data_ptr(), q.data_ptr(), 2, 1100,
-                                                10, 0, 4, q.data_ptr(), None))
+                                                10, 0, 8, q.data_ptr(), None))
+    with pytest.raises(CudaDTWError):  # the two path modes exclude each other
+        handle._check(handle._lib.cdtw_pair_fwd(handle._h, q.data_ptr(), q.data_ptr(), 2, 1100,
+                                                10, 0, 6, q.data_ptr(), q.data_ptr()))
