@@ -285,7 +285,8 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
                 "e2e": {"value": e2e, "unit": "GCUPS",
                         "h2d_bytes_per_step": len(bands) * (x.nbytes + q.nbytes),
                         "d2h_bytes_per_step": len(bands) * nw * 4},
-                "roofline": {"bound": "alu", "kernel": "cdtw_reg2_kernel",
+                "roofline": {"bound": "alu",
+                             "kernel": "cdtw_reg4_kernel (W=12) + cdtw_reg2_kernel (W=25)",
                              "achieved": ach, "peak": peak / 1e9, "unit": "GCUPS",
                              "frac": ach / (peak / 1e9),
                              # DRAM bytes (read + write) of one cdtw_reg2_kernel launch
@@ -321,9 +322,10 @@ def subresults(h, dev) -> dict:
       FP64 oracle's distance at the reported window and the relative error,
       and, on the same inputs, the location and wall time of the reference's
       UCR_DTW_BIN on the host cores.
-    * batched_search: a 128-query sample of config 2 (2^24 ECG-like stream,
+    * batched_search: the 512 queries of config 2 (2^24 ECG-like stream,
       M ~ U{64..1024}, P in {5,10,20}) as one batched graph call, against the
-      same queries as 128 plain searches on the same GPU.
+      same queries as 512 plain searches on the same GPU, with the cDTW cells
+      the plain path computes per query class and their time floor.
     * pair_fwd_bwd: config 3 (4096 pairs, L=256, W=25, z-normalised random
       walks) and its L=2048/W=409 variant: forward (D only), forward with the
       path record, backward, and their ratio; CUDA-graph replays, device time.
@@ -402,27 +404,42 @@ def subresults(h, dev) -> dict:
     # -- batched vs plain ----------------------------------------------------
     x = synth.ecg_like(1 << 24, seed=0)
     dx = torch.from_numpy(x).to(dev)
-    batch = synth.batch_queries(x, 512)[::4]  # every 4th of the 512: 128 queries
+    batch = synth.batch_queries(x, 512)  # the 512 queries of the batched configuration
     qs = [b[0] for b in batch]
     ws = [b[1] for b in batch]
     h.search_batched(dx, qs, ws)  # builds and replays the graph once
     tb, (bl, bd) = dev_time(lambda: h.search_batched(dx, qs, ws))
-    stats = {}
-    for m in sorted({q.size for q in qs}):
-        stats[m] = h.avg_std(dx, m)
 
-    def plain():
+    def plain(counts=None):
         res = []
         for q, w in zip(qs, ws):
-            avg, std = stats[q.size]
+            avg, std = h.avg_std(dx, q.size)
             h.set_query(q, w)
             res.append(h.prune_cdtw(dx, avg, std))
+            if counts is not None:
+                counts.append(h.search_counts())
         return res
-    tp, pres = dev_time(plain)
+    counts = []
+    tp, pres = dev_time(lambda: plain(counts))
     same = sum(int(a == r[0]) for a, r in zip(bl, pres))
+    # cDTW cells the plain path computes at most (windows reaching the cDTW
+    # stage x band cells; early abandoning cuts some), per query class, and
+    # the time they need at the headline kernels' cell rate: the floor of any
+    # schedule that computes them
+    classes = {}
+    for q, w, (_, _, ndtw), b in zip(qs, ws, counts, batch):
+        key = f"M{64 * ((q.size - 1) // 320)}-{64 * ((q.size - 1) // 320) + 319}_P{b[2]}"
+        c = classes.setdefault(key, {"queries": 0, "dtw_windows": 0, "cells": 0.0})
+        c["queries"] += 1
+        c["dtw_windows"] += int(ndtw)
+        c["cells"] += float(ndtw) * cells(q.size, w)
+    tot_cells = sum(c["cells"] for c in classes.values())
     out["batched_search"] = {"queries": len(qs), "stream": "ecg 2^24", "batched_s": tb,
                              "plain_s": tp, "speedup": tp / tb, "same_location": same,
-                             "note": "plain excludes the per-length statistics (shared)"}
+                             "plain_cdtw_cells": tot_cells,
+                             "cell_floor_s_at_7800_gcups": tot_cells / 7.8e12,
+                             "classes": classes,
+                             "note": "plain includes the per-length statistics"}
     del dx
     # many short queries on a short stream: the regime where the per-search
     # launches and host round trips of the plain path dominate
@@ -433,13 +450,38 @@ def subresults(h, dev) -> dict:
     ws = [b[1] for b in batch]
     h.search_batched(dx, qs, ws)
     tb, (bl, bd) = dev_time(lambda: h.search_batched(dx, qs, ws))
-    stats = {m: h.avg_std(dx, m) for m in sorted({q.size for q in qs})}
     tp, pres = dev_time(plain)
     same = sum(int(a == r[0]) for a, r in zip(bl, pres))
     out["batched_search_short"] = {"queries": len(qs), "stream": "ecg 2^20", "M": [64, 128],
                                    "batched_s": tb, "plain_s": tp, "speedup": tp / tb,
                                    "same_location": same}
     del dx
+
+    # -- search over a stream pushed in pieces (host buffers) ---------------
+    x = synth.metal_like(1 << 25, seed=1)
+    q, off = synth.cut_query(x, 256, seed=100 + 256 + 10, noise=0.1)
+    w = synth.band_from_percent(256, 10)
+    xp = torch.from_numpy(x).pin_memory().numpy()
+
+    def streamed():
+        h.stream_begin(q, w)
+        for a in range(0, x.size, 1 << 22):
+            h.stream_push(xp[a:a + (1 << 22)])
+        return h.stream_end()
+    streamed()
+    h.search_host(q, x, w)
+    t0 = time.perf_counter()
+    sl, sd, _ = streamed()
+    ts = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    hl, hd = h.search_host(q, x, w)
+    th = time.perf_counter() - t0
+    out["stream_search"] = {"stream": "metal 2^25 (host, pinned)", "M": 256, "P": 10, "W": w,
+                            "chunk_samples": 1 << 23, "pieces": 8, "streamed_s": ts,
+                            "whole_host_search_s": th, "location": int(sl),
+                            "same_location": int(sl) == int(hl),
+                            "samples_per_s": x.size / ts}
+    del xp
 
     # -- pair forward / backward ------------------------------------------
     pair = {}
@@ -548,8 +590,9 @@ def refine_subresult(h, dev) -> dict:
 
 def profile_case(name: str) -> None:
     """One small run of a scope row (twice, untimed) for an ncu capture:
-    search = config-1 pruned search (2^25 metal-like, M=512, P=10); strip =
-    all-windows cDTW of 2^18 windows at M=1024, W=204 (strip kernel);
+    search = config-1 pruned search (2^25 metal-like, M=512, P=10); strip /
+    wide = all-windows cDTW of 2^18 windows at M=1024, W=204 (strip kernel /
+    lane-group kernel);
     batch_short = the batched search of 512 queries (M 64-128) on a 2^20 ECG-like
     stream; topk =
     top-1000 of one M=256 template on a 2^22 ECG-like stream; pair = 256 pairs
@@ -579,12 +622,15 @@ def profile_case(name: str) -> None:
                 dx = torch.from_numpy(x).to(dev)
                 batch = synth.batch_queries(x, 512, seed=3, m_lo=64, m_hi=128)
                 h.search_batched(dx, [b[0] for b in batch], [b[1] for b in batch])
-            elif name == "strip":
+            elif name in ("strip", "wide"):
+                # all-windows cDTW of 2^18 windows at M=1024, W=204: the strip
+                # kernel ("strip") or the lane-group kernel ("wide")
                 x = synth.metal_like((1 << 18) + 1023, seed=1)
                 dx = torch.from_numpy(x).to(dev)
                 q, _ = synth.cut_query(x, 1024, seed=5, noise=0.1)
                 avg, std = h.avg_std(dx, 1024)
                 h.set_query(q, 204)
+                h.set_band_variant(204, 204, "strip16" if name == "strip" else "lane")
                 h.gpu_cdtw(dx, avg, std)
             elif name == "pair":
                 for n, L, W in ((256, 2048, 409), (4096, 256, 25)):
@@ -595,7 +641,8 @@ def profile_case(name: str) -> None:
                                          .astype(np.float32)).to(dev)
                     path = torch.empty(h.pair_path_bytes(n, L), dtype=torch.uint8, device=dev)
                     h.pair_fwd(q, s, W)
-                    h.pair_fwd(q, s, W, path=path)
+                    h.pair_fwd(q, s, W, path=path, mode="store")
+                    h.pair_fwd(q, s, W, path=path, mode="recompute")
                     h.pair_bwd(q, s, path)
             elif name == "refine":
                 x = synth.ecg_like(1 << 20, seed=0)
@@ -632,7 +679,7 @@ def main() -> None:
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--profile",
-                    choices=["search", "topk", "pair", "refine", "strip", "batch_short"],
+                    choices=["search", "topk", "pair", "refine", "strip", "wide", "batch_short"],
                     help="run one small case of that row twice (for ncu) and exit")
     ap.add_argument("--no-sub", action="store_true",
                     help="skip the pruned / batched search and pair fwd/bwd sub-results")
