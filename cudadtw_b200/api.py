@@ -318,10 +318,11 @@ class Handle:
     # -- batched search ---------------------------------------------------------
     def search_batched(self, subject: torch.Tensor, queries, bands, metric=EUCLIDEAN,
                        rows=None, tiles=None):
-        """Best match (locations, distances) of every query in one graph launch
-        of the persistent batched search.  ``queries``: list of 1-D arrays,
-        ``bands``: W per query; ``rows`` / ``tiles``: per-query tile shape
-        (None = built-in rule; the autotuner fills them per bucket)."""
+        """Best match (locations, distances) of every query in one graph
+        launch.  ``queries``: list of 1-D arrays, ``bands``: W per query.
+        Without ``rows`` / ``tiles``: concurrent single-query pipelines
+        (results bit-identical to prune_cdtw); with them (the autotuner fills
+        them per bucket): the persistent (query, stream-tile) kernels."""
         _dev(subject, torch.float32, "subject")
         qs = [np.ascontiguousarray(q, dtype=np.float32) for q in queries]
         nq = len(qs)

@@ -278,6 +278,22 @@ extern "C" int cdtw_search_batched(cdtw_handle h, const float* d_subject, int64_
         return set_error(h, CDTW_EINVAL, "null pointer or empty batch");
     if (metric != CDTW_EUCLIDEAN && metric != CDTW_MANHATTAN)
         return set_error(h, CDTW_EINVAL, "bad metric %d", metric);
+    if (!rows && !tiles) {
+        // no tile shapes: concurrent single-query pipelines (batch_pipe.cu)
+        std::vector<int> M(Ms, Ms + nq), W(nq);
+        for (int q = 0; q < nq; ++q) {
+            if (M[q] < 11 || M[q] > CDTW_MAX_QUERY || M[q] > N)
+                return set_error(h, CDTW_EINVAL, "query %d: length %d outside [11, min(%d, N)]",
+                                 q, M[q], CDTW_MAX_QUERY);
+            if (Ws[q] < 0) return set_error(h, CDTW_EINVAL, "query %d: negative band", q);
+            W[q] = std::min(Ws[q], M[q] - 1);
+        }
+        if (N - 1 > INT32_MAX) return set_error(h, CDTW_EUNSUPPORTED, "subject too long");
+        CDTW_CUDA(h, cudaSetDevice(h->device));
+        return search_batched_pipelines(h, d_subject, N, h_queries, M, W, metric, locations,
+                                        distances);
+    }
+    batch_pipe_release(h);  // the pipelines plan and this one share the memory budget
     std::vector<int> M(Ms, Ms + nq), W(nq), R(nq), T(nq);
     for (int q = 0; q < nq; ++q) {
         if (M[q] < 11 || M[q] > 4096 || M[q] > N)

@@ -100,11 +100,14 @@ env_window_kernel(const float* __restrict__ x, int64_t N, int W, int T, float2* 
     if (gate && *(const volatile int*)gate <= gate_max) return;  // not needed by this search
     const int K = 2 * W + 1;
     const int S = T + 2 * W;
+    const int64_t ntiles = (N + T - 1) / T;
+    // persistent blocks over the tiles (a gated launch costs one wave)
+    for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
     float* lo = esm;
     float* hi = esm + S;
     float* lo2 = esm + 2 * S;  // PING only
     float* hi2 = esm + 3 * S;
-    const int64_t t0 = (int64_t)blockIdx.x * T;
+    const int64_t t0 = tile * T;
     for (int i = threadIdx.x; i < S; i += kEnvThreads) {
         const int64_t g = t0 - W + i;
         const bool in = g >= 0 && g < N;
@@ -152,6 +155,8 @@ env_window_kernel(const float* __restrict__ x, int64_t N, int W, int T, float2* 
         if (t0 + t >= N) break;
         const int c = t + K - p;
         env[t0 + t] = make_float2(fminf(lo[t], lo[c]), fmaxf(hi[t], hi[c]));
+    }
+    __syncthreads();  // the next tile restages the buffers
     }
 }
 
@@ -226,12 +231,16 @@ int launch_stream_envelope(cdtw_handle h, const float* x, int64_t N, int W, floa
     const size_t smem = (size_t)arrays * (T + 2 * W) * sizeof(float);
     const void* k = ping ? (const void*)env_window_kernel<true> : (const void*)env_window_kernel<false>;
     CDTW_CUDA(h, cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int per_sm = 0;
+    CDTW_CUDA(h, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kEnvThreads, smem));
+    const unsigned grid = (unsigned)std::max<int64_t>(
+        1, std::min<int64_t>(div_up(N, T), (int64_t)std::max(per_sm, 1) * h->sm_count));
     if (ping)
-        env_window_kernel<true><<<(unsigned)div_up(N, T), kEnvThreads, smem, h->stream>>>(
-            x, N, W, T, env, gate, gate_max);
+        env_window_kernel<true><<<grid, kEnvThreads, smem, h->stream>>>(x, N, W, T, env, gate,
+                                                                       gate_max);
     else
-        env_window_kernel<false><<<(unsigned)div_up(N, T), kEnvThreads, smem, h->stream>>>(
-            x, N, W, T, env, gate, gate_max);
+        env_window_kernel<false><<<grid, kEnvThreads, smem, h->stream>>>(x, N, W, T, env, gate,
+                                                                        gate_max);
     CDTW_LAUNCH(h, "env_window_kernel");
     return CDTW_OK;
 }

@@ -27,7 +27,8 @@ int check_cuda(cdtw_handle h, cudaError_t e, const char* what) {
 
 int check_memory_limit(cdtw_handle h, size_t freed, size_t bytes, const char* what) {
     if (h->mem_limit == 0) return CDTW_OK;
-    const size_t held = h->ws_bytes + h->qmem_bytes + h->ring_bytes + h->batch_bytes;
+    const size_t held =
+        h->ws_bytes + h->qmem_bytes + h->ring_bytes + h->batch_bytes + h->stream_bytes;
     if (held - std::min(held, freed) + bytes <= h->mem_limit) return CDTW_OK;
     return set_error(h, CDTW_ENOMEM,
                      "%s needs %zu bytes of device memory: above the handle's limit of %zu "
@@ -63,8 +64,9 @@ struct Carver {
     }
 };
 
-static int ensure_query_mem(cdtw_handle h, int M, int W) {
-    QueryPack& q = h->q;
+}  // namespace cdtw
+
+size_t cdtw::query_pack_layout(int M, int W, QueryPack* q, char* base) {
     const int lq = qpad_len(M, W);
     Carver c;
     const size_t o_qpad = c.take<float>(4 * (size_t)lq);
@@ -74,7 +76,26 @@ static int ensure_query_mem(cdtw_handle h, int M, int W) {
     const int lqr = qrev_len(M, W);
     const size_t o_qrev = c.take<float>(4 * (size_t)lqr);
     const size_t o_qraw = c.take<float>(M);
-    const size_t bytes = c.off;
+    if (q && base) {
+        q->M = M;
+        q->W = W;
+        q->lq = lq;
+        q->qpad = (float*)(base + o_qpad);
+        q->env = (float2*)(base + o_env);
+        q->zq = (float*)(base + o_zq);
+        q->zq64 = (double*)(base + o_zq64);
+        q->lqr = lqr;
+        q->qrev_base = qrev_hi(M, W);
+        q->qrev = (float*)(base + o_qrev);
+        q->qraw = (float*)(base + o_qraw);
+    }
+    return c.off;
+}
+
+namespace cdtw {
+
+static int ensure_query_mem(cdtw_handle h, int M, int W) {
+    const size_t bytes = query_pack_layout(M, W, nullptr, nullptr);
     if (bytes > h->qmem_bytes) {
         CDTW_TRY(check_memory_limit(h, h->qmem_bytes, bytes, "query pack"));
         if (h->qmem) {
@@ -86,18 +107,7 @@ static int ensure_query_mem(cdtw_handle h, int M, int W) {
         CDTW_CUDA(h, cudaMalloc(&h->qmem, bytes));
         h->qmem_bytes = bytes;
     }
-    char* base = (char*)h->qmem;
-    q.M = M;
-    q.W = W;
-    q.lq = lq;
-    q.qpad = (float*)(base + o_qpad);
-    q.env = (float2*)(base + o_env);
-    q.zq = (float*)(base + o_zq);
-    q.zq64 = (double*)(base + o_zq64);
-    q.lqr = lqr;
-    q.qrev_base = qrev_hi(M, W);
-    q.qrev = (float*)(base + o_qrev);
-    q.qraw = (float*)(base + o_qraw);
+    query_pack_layout(M, W, &h->q, (char*)h->qmem);
     return CDTW_OK;
 }
 
@@ -176,6 +186,7 @@ int cdtw_destroy(cdtw_handle h) {
     cudaStreamSynchronize(h->stream);
     if (h->own_stream) cudaStreamSynchronize(h->own_stream);
     batch_plan_release(h);
+    batch_pipe_release(h);
     stream_release(h);
     if (h->ws) cudaFree(h->ws);
     if (h->qmem) cudaFree(h->qmem);

@@ -66,6 +66,8 @@ struct cdtw_handle_s {
     void* batch = nullptr;
     // state of an incremental search over a stream (stream.cu)
     void* stream_state = nullptr;
+    // cached plan of the batched search through concurrent pipelines (batch_pipe.cu)
+    void* batch_pipe = nullptr;
     // boundary rings of the strip kernel's resident warps (grow-only)
     void* ring = nullptr;
     size_t ring_bytes = 0;
@@ -77,6 +79,7 @@ struct cdtw_handle_s {
     // cap on the device memory the handle holds (0: none), cdtw_set_memory_limit
     size_t mem_limit = 0;
     size_t batch_bytes = 0;  // device memory of the cached batched-search plan
+    size_t stream_bytes = 0;  // device memory kept by the streaming search
     // small pinned host buffer for scalar results
     void* pinned = nullptr;
     // stage counts of the last search: windows, after LB_Kim, after LB_Keogh
@@ -98,8 +101,16 @@ struct cdtw_handle_s {
 namespace cdtw {
 
 int set_error(cdtw_handle h, int status, const char* fmt, ...);
+// Bytes of a query pack for (M, W); with q and base, points q's arrays into
+// base (device memory of at least that many bytes).
+size_t query_pack_layout(int M, int W, QueryPack* q, char* base);
 void batch_plan_release(cdtw_handle h);
 void stream_release(cdtw_handle h);
+void batch_pipe_release(cdtw_handle h);
+int search_batched_pipelines(cdtw_handle h, const float* d_subject, int64_t N,
+                             const float* h_queries, const std::vector<int>& M,
+                             const std::vector<int>& W, int metric, int64_t* locations,
+                             float* distances);
 // top-k non-overlapping matches (search.cu)
 size_t topk_workspace_bytes(int64_t N, int M, int W);
 int run_topk(cdtw_handle h, const float* x, int64_t N, const double* mu, const float* sigma,

@@ -152,18 +152,40 @@ __global__ void seeds_to_cands_kernel(const unsigned long long* __restrict__ see
 __global__ void __launch_bounds__(256)
 compact_kim_kernel(const float* __restrict__ lbkim, int Nw, const unsigned long long* key,
                    int* __restrict__ q1, int* __restrict__ n1) {
+    // a lane tests four consecutive windows (one 16-byte load; lbkim is
+    // 256-byte aligned), a warp reserves its survivors with one atomic
     const float bsf = load_bsf(key);
     const int lane = threadIdx.x & 31;
-    for (int base = (blockIdx.x * blockDim.x + threadIdx.x) & ~31; base < Nw;
-         base += gridDim.x * blockDim.x) {
-        const int w = base + lane;
-        const bool keep = w < Nw && lbkim[w] * kLbSlack < bsf;
-        const unsigned m = __ballot_sync(0xffffffffu, keep);
-        if (!m) continue;
+    const int nvec = (Nw + 3) >> 2;
+    const int stride = gridDim.x * blockDim.x;
+    for (int base = (blockIdx.x * blockDim.x + threadIdx.x) & ~31; base < nvec; base += stride) {
+        const int v = base + lane;
+        const int64_t w0 = 4 * (int64_t)v;
+        float4 f = make_float4(INFINITY, INFINITY, INFINITY, INFINITY);
+        if (w0 + 3 < Nw) {
+            f = __ldg(reinterpret_cast<const float4*>(lbkim) + v);
+        } else if (w0 < Nw) {
+            f.x = lbkim[w0];
+            if (w0 + 1 < Nw) f.y = lbkim[w0 + 1];
+            if (w0 + 2 < Nw) f.z = lbkim[w0 + 2];
+        }
+        const unsigned k = (f.x * kLbSlack < bsf ? 1u : 0u) | (f.y * kLbSlack < bsf ? 2u : 0u) |
+                           (f.z * kLbSlack < bsf ? 4u : 0u) | (f.w * kLbSlack < bsf ? 8u : 0u);
+        const int c = __popc(k);
+        int pre = c;  // inclusive prefix over the lanes
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int t = __shfl_up_sync(0xffffffffu, pre, o);
+            if (lane >= o) pre += t;
+        }
+        const int tot = __shfl_sync(0xffffffffu, pre, 31);
+        if (!tot) continue;
         int at = 0;
-        if (lane == 0) at = atomicAdd(n1, __popc(m));
-        at = __shfl_sync(0xffffffffu, at, 0);
-        if (keep) q1[at + __popc(m & ((1u << lane) - 1))] = w;
+        if (lane == 31) at = atomicAdd(n1, tot);
+        at = __shfl_sync(0xffffffffu, at, 31) + pre - c;
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+            if (k & (1u << j)) q1[at++] = (int)w0 + j;
     }
 }
 

@@ -13,6 +13,7 @@
 // and two device buffers alternate, so the copy of one chunk overlaps the
 // search of the previous one.  Windows are numbered globally: chunk k's
 // windows start at k*C - (M-1) (chunk 0's at 0); ties keep the earliest.
+// The buffers outlive a stream and serve the next one when large enough.
 #include "common.cuh"
 
 #include <algorithm>
@@ -42,20 +43,37 @@ struct StreamState {
     char* sws = nullptr;     // search workspace of one chunk
     StreamBest* best = nullptr;
     void* dmem = nullptr;    // one device allocation for all of the above
+    size_t dbytes = 0;       // its size
+    int64_t scap = 0;        // floats per staging buffer
     cudaStream_t copy = nullptr;
     cudaEvent_t staged[2] = {nullptr, nullptr};  // H2D from stage[b] done
     cudaEvent_t done[2] = {nullptr, nullptr};    // search over dbuf[b] done
     cudaEvent_t copied[2] = {nullptr, nullptr};  // dbuf[b] filled (halo + chunk)
+    bool active = false;     // between begin and end
     int64_t fill = 0;        // samples in the current staging buffer
     int64_t chunks = 0;      // chunks launched
     int64_t total = 0;       // samples pushed
     int cur = 0;             // current staging / device buffer
     bool used[2] = {false, false};
 
-    void release() {
-        if (copy) cudaStreamSynchronize(copy);
+    // Ends a stream; the buffers, events and copy stream stay for the next.
+    void finish() {
+        active = false;
+        fill = chunks = total = 0;
+        cur = 0;
+        used[0] = used[1] = false;
+    }
+    void free_stage() {
         for (int b = 0; b < 2; ++b) {
             if (stage[b]) cudaFreeHost(stage[b]);
+            stage[b] = nullptr;
+        }
+        scap = 0;
+    }
+    void release() {
+        if (copy) cudaStreamSynchronize(copy);
+        free_stage();
+        for (int b = 0; b < 2; ++b) {
             if (staged[b]) cudaEventDestroy(staged[b]);
             if (done[b]) cudaEventDestroy(done[b]);
             if (copied[b]) cudaEventDestroy(copied[b]);
@@ -139,6 +157,7 @@ void stream_release(cdtw_handle h) {
         delete s;
         h->stream_state = nullptr;
     }
+    h->stream_bytes = 0;
 }
 
 }  // namespace cdtw
@@ -160,11 +179,19 @@ int cdtw_stream_begin(cdtw_handle h, const float* h_query, int M, int W, int met
     if (C < M || C + M > INT32_MAX)
         return set_error(h, CDTW_EINVAL, "chunk of %lld samples for M=%d", (long long)C, M);
     CDTW_CUDA(h, cudaSetDevice(h->device));
-    stream_release(h);
+    StreamState* s = state(h);
+    if (s && s->active) {
+        // a stream that was begun and never ended: its work is dropped
+        CDTW_CUDA(h, cudaStreamSynchronize(h->stream));
+        CDTW_CUDA(h, cudaStreamSynchronize(s->copy));
+    }
+    if (s) s->finish();
     CDTW_TRY(cdtw_set_query(h, h_query, M, W, CDTW_HOST));
-    StreamState* s = new (std::nothrow) StreamState();
-    if (!s) return set_error(h, CDTW_ENOMEM, "stream state");
-    h->stream_state = s;
+    if (!s) {
+        s = new (std::nothrow) StreamState();
+        if (!s) return set_error(h, CDTW_ENOMEM, "stream state");
+        h->stream_state = s;
+    }
     s->M = M;
     s->W = std::min(W, M - 1);
     s->metric = metric;
@@ -180,26 +207,47 @@ int cdtw_stream_begin(cdtw_handle h, const float* h_query, int M, int W, int met
     const size_t o_mu = take(sizeof(double) * Nw), o_sg = take(sizeof(float) * Nw);
     const size_t o_best = take(sizeof(StreamBest));
     const size_t o_ws = take(search_workspace_bytes(N, M, s->W));
-    int st = check_memory_limit(h, 0, off, "stream buffers");
-    if (st == CDTW_OK) st = check_cuda(h, cudaMalloc(&s->dmem, off), "cudaMalloc(stream)");
+    // buffers of an earlier stream are reused when large enough (its work
+    // has finished: the end of a stream synchronises)
+    int st = CDTW_OK;
+    if (s->dbytes < off) {
+        st = check_memory_limit(h, s->dbytes, off, "stream buffers");
+        if (st == CDTW_OK && s->dmem) {
+            st = check_cuda(h, cudaFree(s->dmem), "cudaFree(stream)");
+            s->dmem = nullptr;
+            s->dbytes = 0;
+            h->stream_bytes = 0;
+        }
+        if (st == CDTW_OK) st = check_cuda(h, cudaMalloc(&s->dmem, off), "cudaMalloc(stream)");
+        if (st == CDTW_OK) {
+            s->dbytes = off;
+            h->stream_bytes = off;
+        }
+    }
+    if (st == CDTW_OK && s->scap < C) {
+        s->free_stage();
+        for (int b = 0; st == CDTW_OK && b < 2; ++b)
+            st = check_cuda(h, cudaMallocHost(&s->stage[b], sizeof(float) * C), "cudaMallocHost");
+        if (st == CDTW_OK) s->scap = C;
+    }
     for (int b = 0; st == CDTW_OK && b < 2; ++b) {
-        st = check_cuda(h, cudaMallocHost(&s->stage[b], sizeof(float) * C), "cudaMallocHost");
-        if (st == CDTW_OK)
+        if (!s->staged[b])
             st = check_cuda(h, cudaEventCreateWithFlags(&s->staged[b], cudaEventDisableTiming),
                             "event");
-        if (st == CDTW_OK)
+        if (st == CDTW_OK && !s->done[b])
             st = check_cuda(h, cudaEventCreateWithFlags(&s->done[b], cudaEventDisableTiming),
                             "event");
-        if (st == CDTW_OK)
+        if (st == CDTW_OK && !s->copied[b])
             st = check_cuda(h, cudaEventCreateWithFlags(&s->copied[b], cudaEventDisableTiming),
                             "event");
     }
-    if (st == CDTW_OK)
+    if (st == CDTW_OK && !s->copy)
         st = check_cuda(h, cudaStreamCreateWithFlags(&s->copy, cudaStreamNonBlocking), "stream");
     if (st != CDTW_OK) {
         stream_release(h);
         return st;
     }
+    s->active = true;
     char* base = (char*)s->dmem;
     s->dbuf[0] = (float*)(base + o_d0);
     s->dbuf[1] = (float*)(base + o_d1);
@@ -219,7 +267,7 @@ int cdtw_stream_begin(cdtw_handle h, const float* h_query, int M, int W, int met
 int cdtw_stream_push(cdtw_handle h, const float* h_samples, int64_t n) {
     if (!h) return CDTW_EINVAL;
     StreamState* s = state(h);
-    if (!s) return set_error(h, CDTW_EINVAL, "no stream begun (cdtw_stream_begin)");
+    if (!s || !s->active) return set_error(h, CDTW_EINVAL, "no stream begun (cdtw_stream_begin)");
     if (n < 0 || (n > 0 && !h_samples)) return set_error(h, CDTW_EINVAL, "bad samples");
     CDTW_CUDA(h, cudaSetDevice(h->device));
     while (n > 0) {
@@ -245,7 +293,7 @@ int cdtw_stream_push(cdtw_handle h, const float* h_samples, int64_t n) {
 int cdtw_stream_end(cdtw_handle h, int64_t* location, float* distance, int64_t* scanned) {
     if (!h) return CDTW_EINVAL;
     StreamState* s = state(h);
-    if (!s) return set_error(h, CDTW_EINVAL, "no stream begun (cdtw_stream_begin)");
+    if (!s || !s->active) return set_error(h, CDTW_EINVAL, "no stream begun (cdtw_stream_begin)");
     CDTW_CUDA(h, cudaSetDevice(h->device));
     int st = CDTW_OK;
     if (s->fill > 0) {
@@ -261,8 +309,11 @@ int cdtw_stream_end(cdtw_handle h, int64_t* location, float* distance, int64_t* 
     if (st == CDTW_OK) memcpy(&b, h->pinned, sizeof(b));
     const int64_t total = s->total;
     const int M = s->M, metric = s->metric;
-    stream_release(h);
-    if (st != CDTW_OK) return st;
+    if (st != CDTW_OK) {
+        stream_release(h);
+        return st;
+    }
+    s->finish();
     if (scanned) *scanned = total;
     if (total < M) return set_error(h, CDTW_EINVAL, "stream of %lld samples is shorter than the query",
                                     (long long)total);

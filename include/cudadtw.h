@@ -172,7 +172,10 @@ int cdtw_search_host(cdtw_handle h, const float* h_query, int M, const float* h_
  * ties keep the earliest window, as UCR_DTW_BIN.cpp:682.  cdtw_stream_end
  * returns the best window, its printed distance (as cdtw_prune_cdtw) and the
  * number of samples scanned, and sets the stage counts and termination flag
- * (cdtw_search_counts / cdtw_search_flag) summed over the chunks. */
+ * (cdtw_search_counts / cdtw_search_flag) summed over the chunks.  The
+ * device and pinned buffers stay with the handle after cdtw_stream_end and
+ * serve the next stream when large enough (freed by cdtw_destroy); a begin
+ * without an end before it drops the unfinished stream. */
 int cdtw_stream_begin(cdtw_handle h, const float* h_query, int M, int W, int metric,
                       int64_t chunk);
 int cdtw_stream_push(cdtw_handle h, const float* h_samples, int64_t n);
@@ -195,20 +198,30 @@ int cdtw_search_flag(cdtw_handle h, int* flag);
 
 /* ---- batched search ------------------------------------------------------------- */
 
-/* Best match of each of nq queries (lengths Ms[q] in [11, 4096], bands Ws[q];
- * the raw float32 values concatenated in h_queries) in one device subject.
- * No reference counterpart: the reference searches one query per process.
- * The whole batch runs as one CUDA graph of persistent kernels that pull
- * (query, stream-tile) work items from device queues: a seed pass (window
- * statistics + LB_Kim per tile), the cDTW of the seed windows, and a main
- * pass (statistics, LB_Kim, LB_Keogh, early-abandoning strip cDTW of the
- * survivors).  rows[q] chooses the main-pass cDTW of the query's (length,
- * band) bucket: 0 = register band (one kernel per W <= 96), 1/2/4/8/16 =
- * strips of that many rows (W >= rows-1); tiles[q] is the windows per work
- * item (a multiple of 32 in [32, 4096]).  NULL selects the built-in rule
- * (register band up to W = 96, 16-row strips above, 1024-window tiles).  The graph is built on the first call and replayed while the subject
- * pointer, N, lengths, bands, shapes and metric stay the same.  Results as
- * cdtw_prune_cdtw: window start (lowest on ties) and printed distance. */
+/* Best match of each of nq queries (lengths Ms[q], bands Ws[q]; the raw
+ * float32 values concatenated in h_queries) in one device subject.  No
+ * reference counterpart: the reference searches one query per process.
+ *
+ * rows == tiles == NULL (lengths up to CDTW_MAX_QUERY): every query runs the
+ * cdtw_prune_cdtw pipeline, spread over 16 internal lanes (stream, query
+ * pack, statistics, work area) that run concurrently, queries of one length
+ * sharing their window statistics; the whole batch is one CUDA graph
+ * (captured on the first call of a shape, replayed while the subject
+ * pointer, N, lengths, bands and metric stay the same), one host sync per
+ * call.  Results are bit-identical to cdtw_prune_cdtw's.
+ *
+ * With rows / tiles (lengths up to 4096): one graph of persistent kernels
+ * that pull (query, stream-tile) work items from device queues: a seed pass
+ * (tile statistics + LB_Kim), the cDTW of the seed windows, and a main pass
+ * (statistics, LB_Kim, LB_Keogh, early-abandoning cDTW of the survivors).
+ * rows[q] chooses the main-pass cDTW of the query's (length, band) bucket:
+ * 0 = register band (one kernel per W <= 96), 1/2/4/8/16 = strips of that
+ * many rows (W >= rows-1); tiles[q] is the windows per work item (a multiple
+ * of 32 in [32, 4096]); either array may be NULL for the built-in choice
+ * (register band up to W = 96, 16-row strips above, 1024-window tiles).
+ *
+ * Results as cdtw_prune_cdtw: window start (lowest on ties) and printed
+ * distance. */
 int cdtw_search_batched(cdtw_handle h, const float* d_subject, int64_t N,
                         const float* h_queries, const int* Ms, const int* Ws, int nq,
                         int metric, const int* rows, const int* tiles, int64_t* locations,

@@ -1,7 +1,9 @@
-"""GPU parity of the batched persistent search: every query's best match
-equals the single-query pruned search (and so the unpruned argmin), across
-mixed lengths, bands, both cell costs and every strip-row choice; repeated
-calls replay the cached graph with new query values."""
+"""GPU parity of the batched search: every query's best match equals the
+single-query pruned search (and so the unpruned argmin) -- bit for bit in the
+concurrent-pipelines mode, to the tile statistics' rounding in the
+persistent-tile mode -- across mixed lengths, bands, both cell costs and
+every strip-row choice, and the FP64 oracle's argmin; repeated calls replay
+the cached graph with new query values."""
 import numpy as np
 import pytest
 import torch
@@ -48,6 +50,33 @@ def test_batched_equals_single_query_search(handle):
     qs2 = [q[::-1].copy() for q in qs]
     locs2, dists2 = handle.search_batched(dx, qs2, ws)
     _check(handle, dx, qs2, ws, locs2, dists2)
+
+
+@pytest.mark.parametrize("metric", [0, 1])
+def test_batched_pipelines_bit_identical_to_single_search(handle, metric):
+    """Without tile shapes every query runs the single-query pipeline in one
+    of the concurrent lanes of the batch graph: locations and distances equal
+    prune_cdtw's exactly, on the first (eager) call, on replays with new
+    query values, and after switching to the tile mode and back.  The batch
+    mixes register-band, lane-group and strip bands and repeated lengths
+    (shared statistics)."""
+    x = synth.ecg_like(200_000, seed=51)
+    batch = synth.batch_queries(x, 40, seed=9, m_lo=64, m_hi=1500)
+    qs = [b[0] for b in batch]
+    ws = [b[1] for b in batch]
+    qs += [qs[3].copy(), synth.random_walk(1600, 5)]
+    ws += [max(1, ws[3] // 2), 800]  # a repeated length; a band above the lane kernels
+    dx = torch.from_numpy(x).cuda()
+
+    def check(qv):
+        locs, dists = handle.search_batched(dx, qv, ws, metric=metric)
+        for q, w, loc, dist in zip(qv, ws, locs, dists):
+            assert (loc, dist) == _single(handle, dx, q, w, metric)
+
+    check(qs)
+    check([q[::-1].copy() for q in qs])  # replay of the captured graph
+    handle.search_batched(dx, qs[:3], ws[:3], metric=metric, rows=[16] * 3)
+    check(qs)
 
 
 @pytest.mark.parametrize("metric", [0, 1])

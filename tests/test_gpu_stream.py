@@ -91,6 +91,33 @@ def test_stream_full_size_metal(handle):
     assert loc == ploc and abs(dist - pdist) <= 1e-5 * pdist
 
 
+def test_stream_buffers_reused_across_streams(handle):
+    """Streams back to back on one handle reuse the buffers of the earlier
+    ones (growing them for a larger chunk or query); a stream begun again
+    before its end drops the unfinished one.  Every result equals the
+    stream's own fresh-handle search, and repeating a stream of the same
+    shape takes no device memory."""
+    from cudadtw_b200 import Handle
+    x = synth.ecg_like(300_000, seed=12)
+    cases = [(128, 12, 0, 65_536), (300, 30, 1, 50_000), (128, 12, 0, 65_536),
+             (700, 70, 0, 131_072)]
+    want = []
+    with Handle(0) as fresh:
+        for m, w, metric, chunk in cases:
+            q, _ = synth.cut_query(x, m, seed=m + w, noise=0.1)
+            want.append(_stream_search(fresh, q, x, w, metric, chunk=chunk, seed=m))
+    q0, _ = synth.cut_query(x, 128, seed=140, noise=0.1)
+    handle.stream_begin(q0, 12, chunk=65_536)
+    handle.stream_push(x[:200_000])  # never ended
+    free = []
+    for (m, w, metric, chunk), ref in zip(cases, want):
+        q, _ = synth.cut_query(x, m, seed=m + w, noise=0.1)
+        assert _stream_search(handle, q, x, w, metric, chunk=chunk, seed=m) == ref
+        torch.cuda.synchronize()
+        free.append(torch.cuda.mem_get_info()[0])
+    assert free[2] == free[1]
+
+
 def test_stream_errors(handle):
     from cudadtw_b200 import CudaDTWError
     q = synth.ecg_like(128, seed=1)
