@@ -579,13 +579,40 @@ def refine_subresult(h, dev) -> dict:
         qq = np.repeat(new[t][None, :], k, axis=0)
         d = oracle.pair_fwdbwd(qq, win, bands[t], znorm=True)[0].mean()
         check.append(abs(d - losses[-1, t]) / d)
-    return {"templates": 64, "k": int(k), "steps": 100, "topk_s": t_topk,
-            "refine_s": t_ref, "ms_per_step": t_ref * 1e3 / 100,
-            "pair_steps_per_s": pairs * 100 / t_ref,
-            "fwd_gcups_equiv": cells_step * 101 / t_ref / 1e9,
-            "loss_first_mean": float(losses[0].mean()), "loss_last_mean": float(losses[-1].mean()),
-            "templates_improved": int(np.sum(losses[-1] < losses[0])),
-            "fp64_recheck_max_rel": float(max(check))}
+    fixed = {"templates": 64, "k": int(k), "steps": 100, "topk_s": t_topk,
+             "refine_s": t_ref, "ms_per_step": t_ref * 1e3 / 100,
+             "pair_steps_per_s": pairs * 100 / t_ref,
+             "fwd_gcups_equiv": cells_step * 101 / t_ref / 1e9,
+             "loss_first_mean": float(losses[0].mean()),
+             "loss_last_mean": float(losses[-1].mean()),
+             "templates_improved": int(np.sum(losses[-1] < losses[0])),
+             "fp64_recheck_max_rel": float(max(check)),
+             "matches": "searched once (cdtw_topk), fixed over the steps"}
+    # config 4 as specified: random-walk templates, the top-1000 matches
+    # searched again on the device at every step inside the one graph
+    temps = [synth.random_walk(int(m), 900 + i) for i, m in enumerate(ms)]
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    new, losses, fin = h.refine_templates_search(dx, temps, bands, 1000, steps=100, lr=1e-2)
+    t_rs = time.perf_counter() - t0
+    check, same = [], 0
+    for t in range(4):
+        win = np.stack([x[s:s + ms[t]] for s in fin[t]]).astype(np.float32)
+        qq = np.repeat(new[t][None, :], 1000, axis=0)
+        d = oracle.pair_fwdbwd(qq, win, bands[t], znorm=True)[0].mean()
+        check.append(abs(d - losses[-1, t]) / d)
+        h.set_query(new[t], bands[t])
+        same += int(np.array_equal(h.topk(dx, *stats[ms[t]], 1000)[0], fin[t]))
+    searched = {"templates": 64, "init": "random walk", "k": 1000, "steps": 100,
+                "refine_s": t_rs, "ms_per_step": t_rs * 1e3 / 101,
+                "loss_per_step_mean": [float(v) for v in losses.mean(axis=1)[::10]],
+                "loss_first_mean": float(losses[0].mean()),
+                "loss_last_mean": float(losses[-1].mean()),
+                "templates_improved": int(np.sum(losses[-1] < losses[0])),
+                "fp64_recheck_max_rel": float(max(check)),
+                "plain_topk_recheck_same_matches": f"{same}/4",
+                "matches": "top-1000 searched on the device at every step, in the graph"}
+    return {"fixed_matches": fixed, "searched_every_step": searched}
 
 
 def profile_case(name: str) -> None:
@@ -597,7 +624,9 @@ def profile_case(name: str) -> None:
     stream; topk =
     top-1000 of one M=256 template on a 2^22 ECG-like stream; pair = 256 pairs
     of L=2048, W=409 and 4096 pairs of L=256, W=25 (forward, forward with path,
-    backward); refine = 8 templates x 200 matches, 5 Adam steps."""
+    backward); refine = 8 templates x 200 matches, 5 Adam steps; refine_search
+    = the same with random-walk templates and the matches searched at every
+    step."""
     import torch
     from cudadtw_b200 import Handle, synth
     dev = torch.device("cuda", 0)
@@ -657,6 +686,12 @@ def profile_case(name: str) -> None:
                     temps.append(q)
                     bands.append(m // 10)
                 h.refine_templates(dx, temps, bands, np.stack(locs), steps=5)
+            elif name == "refine_search":
+                x = synth.ecg_like(1 << 20, seed=0)
+                dx = torch.from_numpy(x).to(dev)
+                temps = [synth.random_walk(128 + 32 * i, 60 + i) for i in range(8)]
+                h.refine_templates_search(dx, temps, [(128 + 32 * i) // 10 for i in range(8)],
+                                          200, steps=5)
             else:
                 raise SystemExit(f"unknown profile case {name}")
             torch.cuda.synchronize()
@@ -679,7 +714,8 @@ def main() -> None:
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--profile",
-                    choices=["search", "topk", "pair", "refine", "strip", "wide", "batch_short"],
+                    choices=["search", "topk", "pair", "refine", "refine_search", "strip", "wide",
+                             "batch_short"],
                     help="run one small case of that row twice (for ncu) and exit")
     ap.add_argument("--no-sub", action="store_true",
                     help="skip the pruned / batched search and pair fwd/bwd sub-results")

@@ -41,6 +41,8 @@ SIGNATURES = {
     "cdtw_stream_end": (c_int, [c_vp, c_i64p, c_f32p, c_i64p]),
     "cdtw_topk": (c_int, [c_vp, c_vp, c_i64, c_vp, c_vp, c_int, c_int, c_vp, c_vp,
                           ctypes.POINTER(c_int)]),
+    "cdtw_topk_device": (c_int, [c_vp, c_vp, c_i64, c_vp, c_vp, c_int, c_int, c_vp, c_vp,
+                                 ctypes.POINTER(c_int)]),
     "cdtw_set_band_variant": (c_int, [c_vp, c_int, c_int, c_int]),
     "cdtw_search_batched": (c_int, [c_vp, c_vp, c_i64, c_vp, c_vp, c_vp, c_int, c_int, c_vp, c_vp,
                                     c_vp, c_vp]),
@@ -56,6 +58,8 @@ SIGNATURES = {
     "cdtw_pair_path_bytes": (ctypes.c_size_t, [c_i64, c_int]),
     "cdtw_refine_templates": (c_int, [c_vp, c_vp, c_i64, c_vp, c_vp, c_vp, c_int, c_vp, c_int,
                                       c_int, ctypes.c_float, c_int, c_vp]),
+    "cdtw_refine_templates_search": (c_int, [c_vp, c_vp, c_i64, c_vp, c_vp, c_vp, c_int, c_int,
+                                             c_int, ctypes.c_float, c_int, c_vp, c_vp]),
     "cdtw_pair_workspace_bytes": (ctypes.c_size_t, [c_i64, c_int, c_int, c_int, c_int]),
     "cdtw_pair_last_mode": (c_int, [c_vp, ctypes.POINTER(c_int)]),
     "cdtw_pair_fwd": (c_int, [c_vp, c_vp, c_vp, c_i64, c_int, c_int, c_int, c_int, c_vp, c_vp]),

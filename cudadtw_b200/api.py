@@ -210,6 +210,17 @@ class Handle:
                                         _ptr(dists), ctypes.byref(found)))
         return locs[:found.value], dists[:found.value]
 
+    def topk_device(self, subject, avg, std, k: int, metric=EUCLIDEAN):
+        """topk with every step on the device (cdtw_topk_device): the same
+        picks, no host round trip before the end."""
+        locs = np.empty(k, np.int64)
+        dists = np.empty(k, np.float32)
+        found = ctypes.c_int()
+        self._check(self._lib.cdtw_topk_device(self._h, _ptr(subject), subject.numel(),
+                                               _ptr(avg), _ptr(std), _metric(metric), int(k),
+                                               _ptr(locs), _ptr(dists), ctypes.byref(found)))
+        return locs[:found.value], dists[:found.value]
+
     # -- search over a stream pushed in pieces ------------------------------
     def stream_begin(self, query, W: int, metric=EUCLIDEAN, chunk: int = 0) -> None:
         """Start a search whose subject arrives by stream_push (chunked copies
@@ -419,3 +430,27 @@ class Handle:
             res.append(out[o:o + m].copy())
             o += m
         return res, losses
+
+    def refine_templates_search(self, subject: torch.Tensor, templates, bands, k: int,
+                                steps: int, lr: float = 1e-2, metric=EUCLIDEAN):
+        """Adam refinement with the top-k matches searched again at every step
+        (cdtw_refine_templates_search, one CUDA graph).  Returns the refined
+        templates, the (steps+1, nt) mean distances to each step's matches,
+        and the (nt, k) matches of the last step."""
+        _dev(subject, torch.float32, "subject")
+        ts = [np.ascontiguousarray(t, dtype=np.float32) for t in templates]
+        nt = len(ts)
+        flat = torch.from_numpy(np.concatenate(ts)).to(subject.device)
+        ms = np.array([t.size for t in ts], dtype=np.int32)
+        ws = np.ascontiguousarray(bands, dtype=np.int32)
+        losses = np.empty((steps + 1, nt), np.float32)
+        locs = np.empty((nt, k), np.int64)
+        self._check(self._lib.cdtw_refine_templates_search(
+            self._h, _ptr(subject), subject.numel(), _ptr(flat), _ptr(ms), _ptr(ws), nt, int(k),
+            int(steps), float(lr), _metric(metric), _ptr(losses), _ptr(locs)))
+        out = flat.cpu().numpy()
+        res, o = [], 0
+        for m in ms:
+            res.append(out[o:o + m].copy())
+            o += m
+        return res, losses, locs

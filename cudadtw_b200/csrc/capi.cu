@@ -441,6 +441,54 @@ int cdtw_topk(cdtw_handle h, const float* d_subject, int64_t N, const double* d_
     return CDTW_OK;
 }
 
+int cdtw_topk_device(cdtw_handle h, const float* d_subject, int64_t N, const double* d_avg,
+                     const float* d_std, int metric, int k, int64_t* locations,
+                     float* distances, int* found) {
+    if (!h) return CDTW_EINVAL;
+    if (found) *found = 0;
+    if (!h->has_query) return set_error(h, CDTW_EINVAL, "no query set (cdtw_set_query)");
+    const int M = h->q.M;
+    if (!d_subject || !d_avg || !d_std || !locations || k < 1)
+        return set_error(h, CDTW_EINVAL, "bad top-k arguments");
+    if (N < M || N - M + 1 > (int64_t)INT32_MAX)
+        return set_error(h, CDTW_EINVAL, "subject length %lld for M=%d", (long long)N, M);
+    if (M < 11) return set_error(h, CDTW_EUNSUPPORTED, "top-k search needs M >= 11");
+    if (!valid_metric(metric)) return set_error(h, CDTW_EINVAL, "bad metric %d", metric);
+    if (k > (N - M + 1)) k = (int)(N - M + 1);
+    CDTW_CUDA(h, cudaSetDevice(h->device));
+    Carver c;
+    const size_t o_ws = c.take<char>(topk_device_workspace_bytes(N, M, h->q.W, k));
+    const size_t o_pk = c.take<int32_t>(k);
+    const size_t o_pd = c.take<float>(k);
+    const size_t o_n = c.take<int>(2);
+    CDTW_TRY(ensure_workspace(h, c.off));
+    char* base = (char*)h->ws;
+    int32_t* picks = (int32_t*)(base + o_pk);
+    float* pick_d = (float*)(base + o_pd);
+    int* cnt = (int*)(base + o_n);
+    CDTW_TRY(run_topk_device(h, d_subject, N, d_avg, d_std, metric == CDTW_EUCLIDEAN, k, k,
+                             base + o_ws, nullptr, nullptr, picks, pick_d, cnt, cnt + 1));
+    int hc[2];
+    std::vector<int32_t> hp(k);
+    std::vector<float> hd(k);
+    CDTW_CUDA(h, cudaMemcpyAsync(hc, cnt, sizeof(hc), cudaMemcpyDeviceToHost, h->stream));
+    CDTW_CUDA(h, cudaMemcpyAsync(hp.data(), picks, sizeof(int32_t) * k, cudaMemcpyDeviceToHost,
+                                 h->stream));
+    CDTW_CUDA(h, cudaMemcpyAsync(hd.data(), pick_d, sizeof(float) * k, cudaMemcpyDeviceToHost,
+                                 h->stream));
+    CDTW_CUDA(h, cudaStreamSynchronize(h->stream));
+    if (hc[1] != 0)
+        return set_error(h, CDTW_EUNSUPPORTED,
+                         "more windows under the top-k threshold than the hit list holds");
+    const int n = std::min(hc[0], k);
+    for (int i = 0; i < n; ++i) {
+        locations[i] = hp[i];
+        if (distances) distances[i] = metric == CDTW_EUCLIDEAN ? sqrtf(hd[i]) : hd[i];
+    }
+    if (found) *found = n;
+    return CDTW_OK;
+}
+
 int cdtw_search_host(cdtw_handle h, const float* h_query, int M, const float* h_subject,
                      int64_t N, int W, int metric, int64_t* location, float* distance) {
     if (!h) return CDTW_EINVAL;

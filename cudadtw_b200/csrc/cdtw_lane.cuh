@@ -62,6 +62,7 @@ struct LaneArgs {
     const int* count;
     int* work;
     unsigned long long* key;
+    HitSink sink;
 };
 
 constexpr int kLaneThreads = 256;
@@ -346,8 +347,8 @@ cdtw_lane_search_kernel(const LaneArgs a) {
         lane_pair_dtw<B, EU, true>(a, lsq4, g, a.x + c0.w, a.x + c1.w, n0, n1, c0.lbk, c1.lbk,
                                    al0, al1, r0, r1);
         if (g == a.gW) {
-            if (i0 < n && r0 < CDTW_INF) atomicMin(a.key, pack_key(r0, (uint32_t)c0.w));
-            if (i1 < n && r1 < CDTW_INF) atomicMin(a.key, pack_key(r1, (uint32_t)c1.w));
+            if (i0 < n && r0 < CDTW_INF) report_window(a.key, a.sink, r0, (uint32_t)c0.w);
+            if (i1 < n && r1 < CDTW_INF) report_window(a.key, a.sink, r1, (uint32_t)c1.w);
         }
     }
 }

@@ -73,20 +73,23 @@ int choose_variant(cdtw_handle h, int W) {
 
 int launch_cdtw_strip_search(cdtw_handle h, const float* x, int64_t N, const double* mu,
                              const float* sigma, const Cand* cands, const int* count, int* work,
-                             int max_count, bool euclid, int R, unsigned long long* key);
+                             int max_count, bool euclid, int R, unsigned long long* key,
+                             const HitSink& sink);
 
 int launch_cdtw_search(cdtw_handle h, const float* x, int64_t N, const double* mu,
                        const float* sigma, const Cand* cands, const int* count, int* work,
-                       int max_count, bool euclid, unsigned long long* key) {
+                       int max_count, bool euclid, unsigned long long* key,
+                       const HitSink& sink) {
     const QueryPack& q = h->q;
     if (max_count <= 0) return CDTW_OK;
     const int variant = choose_variant(h, q.W);
     if (variant == CDTW_VARIANT_LANE)
         return launch_cdtw_lane_search(h, x, N, mu, sigma, cands, count, work, max_count, euclid,
-                                       key);
+                                       key, sink);
     if (variant != CDTW_VARIANT_REGISTER)
         return launch_cdtw_strip_search(h, x, N, mu, sigma, cands, count, work, max_count,
-                                        euclid, variant == CDTW_VARIANT_STRIP16 ? 16 : 32, key);
+                                        euclid, variant == CDTW_VARIANT_STRIP16 ? 16 : 32, key,
+                                        sink);
     RegSearchKernel k = euclid ? reg_kernels().seu[q.W] : reg_kernels().smh[q.W];
     const int lq4 = q.lq / 4;
     const size_t smem = (size_t)q.lq * 4 * sizeof(float) + (size_t)q.M * sizeof(float2);
@@ -99,7 +102,7 @@ int launch_cdtw_search(cdtw_handle h, const float* x, int64_t N, const double* m
     const unsigned blocks = (unsigned)std::max<int64_t>(
         1, std::min<int64_t>(want, (int64_t)std::max(per_sm, 1) * h->sm_count));
     k<<<blocks, kRegBlock, smem, h->stream>>>(x, mu, sigma, (const float4*)q.qpad, lq4, q.env,
-                                              q.M, cands, count, work, key);
+                                              q.M, cands, count, work, key, sink);
     CDTW_LAUNCH(h, "cdtw_reg_search_kernel");
     return CDTW_OK;
 }

@@ -333,14 +333,15 @@ __device__ __forceinline__ float reg_window_dtw(const float4* sq4, int lq4,
 // Search variant: persistent warps take 32 candidates at a time from a device
 // list, skip those whose lower bound already exceeds the best-so-far, run the
 // register-band DTW with early abandoning, and fold results into *key by a
-// packed (distance, window) atomicMin, so ties keep the lowest window.
+// packed (distance, window) atomicMin, so ties keep the lowest window (or
+// append them to a hit list, report_window).
 template <int W, bool EU>
 __global__ void __launch_bounds__(kRegBlock)
 cdtw_reg_search_kernel(const float* __restrict__ x, const double* __restrict__ mu,
                        const float* __restrict__ sigma, const float4* __restrict__ qpad4, int lq4,
                        const float2* __restrict__ qenv, int M, const Cand* __restrict__ cands,
                        const int* __restrict__ count, int* __restrict__ work,
-                       unsigned long long* __restrict__ key) {
+                       unsigned long long* __restrict__ key, const HitSink sink) {
     extern __shared__ float4 sq4[];
     float2* senv = (float2*)(sq4 + 4 * lq4);
     for (int e = threadIdx.x; e < 4 * lq4; e += blockDim.x) sq4[e] = qpad4[e];
@@ -363,7 +364,7 @@ cdtw_reg_search_kernel(const float* __restrict__ x, const double* __restrict__ m
         if (!__any_sync(0xffffffffu, alive)) continue;
         const Norm nm = make_norm(mu[c.w], sigma[c.w]);
         const float res = reg_window_dtw<W, EU>(sq4, lq4, senv, M, x + c.w, nm, c.lbk, alive, key);
-        if (i < n && res < CDTW_INF) atomicMin(key, pack_key(res, (uint32_t)c.w));
+        if (i < n && res < CDTW_INF) report_window(key, sink, res, (uint32_t)c.w);
     }
 }
 
@@ -371,7 +372,7 @@ using RegKernel = void (*)(const float*, const double*, const float*, const floa
                            int, const int32_t*, int, float*);
 using RegSearchKernel = void (*)(const float*, const double*, const float*, const float4*, int,
                                  const float2*, int, const Cand*, const int*, int*,
-                                 unsigned long long*);
+                                 unsigned long long*, const HitSink);
 
 // Instantiates the kernels for bands LO..HI into the dispatch tables.
 template <int LO, int HI>

@@ -39,7 +39,8 @@ template <int R, bool EU>
 __global__ void __launch_bounds__(kStripWarps * 32)
 cdtw_strip_search_kernel(const StripArgs a, const float2* __restrict__ qenv,
                          const Cand* __restrict__ cands, const int* __restrict__ count,
-                         int* __restrict__ work, unsigned long long* __restrict__ key) {
+                         int* __restrict__ work, unsigned long long* __restrict__ key,
+                         const HitSink sink) {
     float* ring = lane_ring(a);
     const int lane = threadIdx.x & 31;
     const int n = *(const volatile int*)count;
@@ -57,7 +58,7 @@ cdtw_strip_search_kernel(const StripArgs a, const float2* __restrict__ qenv,
         bool alive = (i < n) && (c.lb * kLbSlack < load_bsf(key));
         if (!__any_sync(0xffffffffu, alive)) continue;
         const float res = strip_dtw<R, EU, true>(a, c.w, ring, qenv, c.lbk, alive, key);
-        if (i < n && res < CDTW_INF) atomicMin(key, pack_key(res, (uint32_t)c.w));
+        if (i < n && res < CDTW_INF) report_window(key, sink, res, (uint32_t)c.w);
     }
 }
 
@@ -129,14 +130,15 @@ int launch_cdtw_strip(cdtw_handle h, const float* x, int64_t N, const double* mu
 
 int launch_cdtw_strip_search(cdtw_handle h, const float* x, int64_t N, const double* mu,
                              const float* sigma, const Cand* cands, const int* count, int* work,
-                             int max_count, bool euclid, int R, unsigned long long* key) {
+                             int max_count, bool euclid, int R, unsigned long long* key,
+                             const HitSink& sink) {
     const QueryPack& q = h->q;
     if (R != 16 && R != 32) return set_error(h, CDTW_EINVAL, "strip rows must be 16 or 32");
     if (q.W < R - 1)
         return set_error(h, CDTW_EUNSUPPORTED, "strip kernel needs W >= R-1 (W=%d R=%d)", q.W, R);
     if (max_count <= 0) return CDTW_OK;
     using SK = void (*)(const StripArgs, const float2*, const Cand*, const int*, int*,
-                        unsigned long long*);
+                        unsigned long long*, const HitSink);
     SK k;
     if (R == 16)
         k = euclid ? cdtw_strip_search_kernel<16, true> : cdtw_strip_search_kernel<16, false>;
@@ -148,7 +150,7 @@ int launch_cdtw_strip_search(cdtw_handle h, const float* x, int64_t N, const dou
     a.idx = nullptr;
     a.L = 0;
     a.out = nullptr;
-    k<<<blocks, kStripWarps * 32, 0, h->stream>>>(a, q.env, cands, count, work, key);
+    k<<<blocks, kStripWarps * 32, 0, h->stream>>>(a, q.env, cands, count, work, key, sink);
     CDTW_LAUNCH(h, "cdtw_strip_search_kernel");
     return CDTW_OK;
 }

@@ -115,6 +115,18 @@ int search_batched_pipelines(cdtw_handle h, const float* d_subject, int64_t N,
 size_t topk_workspace_bytes(int64_t N, int M, int W);
 int run_topk(cdtw_handle h, const float* x, int64_t N, const double* mu, const float* sigma,
              bool euclid, int k, char* ws_base, std::vector<unsigned long long>* picks);
+// the same with every step on the device (graph-capturable); k2 >= k picks
+size_t topk_device_workspace_bytes(int64_t N, int M, int W, int k2);
+int run_topk_device(cdtw_handle h, const float* x, int64_t N, const double* mu,
+                    const float* sigma, bool euclid, int k, int k2, char* ws_base,
+                    const int32_t* prev, const int* prev_n, int32_t* picks, float* pick_d,
+                    int* npicks, int* status);
+// topk_device.cu
+int launch_topk_threshold(cdtw_handle h, const float* sd, int nseg, const float* prev_d,
+                          const int* prev_n, int k2, unsigned long long* key, float* t_out);
+int launch_topk_greedy(cdtw_handle h, const unsigned long long* hits, const int* nh, int cap,
+                       int k2, int M, int* acc, int32_t* picks, float* pick_d, int* npicks,
+                       int* status);
 // pairwise cDTW forward / backward (pair.cu)
 void pair_shape(int L, int W, int* G, int* C);
 size_t pair_dirs_words(int L, int W);
@@ -297,6 +309,30 @@ __device__ __forceinline__ float load_bsf(const unsigned long long* key) {
     return (k == ~0ull) ? CDTW_INF : d;
 }
 
+// Where a search kernel puts a finished window: without a hit list, the
+// packed (distance, window) atomicMin into *key (argmin search); with one,
+// every window whose packed key is below *key is appended to the list (the
+// key then holds a fixed threshold that also drives the early abandoning:
+// top-k candidate collection).  Appends past cap are counted, not stored.
+struct HitSink {
+    unsigned long long* hits = nullptr;
+    int* n = nullptr;
+    int cap = 0;
+};
+
+__device__ __forceinline__ void report_window(unsigned long long* key, const HitSink& s,
+                                              float res, uint32_t w) {
+    const unsigned long long k = pack_key(res, w);
+    if (!s.hits) {
+        atomicMin(key, k);
+        return;
+    }
+    if (k < *(const volatile unsigned long long*)key) {
+        const int at = atomicAdd(s.n, 1);
+        if (at < s.cap) s.hits[at] = k;
+    }
+}
+
 // ---- kernel launchers (defined in the .cu files) ----------------------------
 
 int launch_avg_std(cdtw_handle h, const float* x, int64_t N, int M, double* mu, float* sigma);
@@ -341,7 +377,8 @@ int launch_cdtw_lane(cdtw_handle h, const float* x, int64_t N, const double* mu,
                      const float* sigma, const int32_t* idx, int64_t L, bool euclid, float* out);
 int launch_cdtw_lane_search(cdtw_handle h, const float* x, int64_t N, const double* mu,
                             const float* sigma, const Cand* cands, const int* count, int* work,
-                            int max_count, bool euclid, unsigned long long* key);
+                            int max_count, bool euclid, unsigned long long* key,
+                            const HitSink& sink);
 // floats per shifted query copy (QueryPack::lq) of a handle's query pack
 inline int qpad_len(int M, int W) { return (int)(((int64_t)M + 2 * W + 56 + 3) / 4 * 4); }
 // Kernel choice for band W: CDTW_VARIANT_REGISTER (one thread per window, band
@@ -362,10 +399,13 @@ int launch_lb_keogh(cdtw_handle h, const float* x, int64_t N, const double* mu,
                     const float* sigma, const float2* xenv, const int32_t* idx, int64_t L,
                     bool euclid, float* fwd, float* rev);
 // DTW over a device candidate list with early abandoning and a fused argmin
-// into *key (packed distance/index).  `count` and `work` are device ints.
+// into *key (packed distance/index), or, with a hit list, the collection of
+// the windows below the threshold in *key.  `count` and `work` are device
+// ints.
 int launch_cdtw_search(cdtw_handle h, const float* x, int64_t N, const double* mu,
                        const float* sigma, const Cand* cands, const int* count, int* work,
-                       int max_count, bool euclid, unsigned long long* key);
+                       int max_count, bool euclid, unsigned long long* key,
+                       const HitSink& sink = HitSink());
 // init_key: a device key the search starts from (a bound carried over from
 // earlier parts of a stream), else no bound.
 int run_search(cdtw_handle h, const float* x, int64_t N, const double* mu, const float* sigma,

@@ -616,6 +616,96 @@ int run_topk(cdtw_handle h, const float* x, int64_t N, const double* mu, const f
     return CDTW_OK;
 }
 
+// Workspace of run_topk_device: that of run_topk plus the re-scored previous
+// picks, the threshold and the accepted-window buckets of the greedy.
+namespace {
+struct TopkDevWs {
+    float* prev_d;
+    float* T;
+    int* acc;
+    int nbuckets;
+};
+size_t carve_topk_device(int64_t N, int M, int W, int k2, SearchWs* sw, TopkWs* tw,
+                         TopkDevWs* dw, char* base) {
+    const int64_t Nw = N - M + 1;
+    size_t off = carve_topk(N, Nw, M, W, topk_cap(Nw), sw, tw, base);
+    auto take = [&](size_t bytes) {
+        const size_t o = off;
+        off = (size_t)round_up((int64_t)(off + bytes), 256);
+        return base ? base + o : nullptr;
+    };
+    dw->prev_d = (float*)take(sizeof(float) * std::max(k2, 1));
+    dw->T = (float*)take(sizeof(float));
+    dw->nbuckets = (int)div_up(Nw, M);
+    dw->acc = (int*)take(sizeof(int) * ((size_t)dw->nbuckets + 2));
+    return off;
+}
+}  // namespace
+
+size_t topk_device_workspace_bytes(int64_t N, int M, int W, int k2) {
+    SearchWs sw;
+    TopkWs tw;
+    TopkDevWs dw;
+    return carve_topk_device(N, M, W, k2, &sw, &tw, &dw, nullptr);
+}
+
+// The top-k search of run_topk with every step on the device (no host
+// synchronisation, so it can be captured in a CUDA graph): the threshold T
+// is selected on the device (and lowered to the largest re-scored distance
+// of `prev`, a previous set of k2 non-overlapping windows, when *prev_n ==
+// k2), the windows at distance <= T are collected by the early-abandoning
+// search kernels into a hit list, and the greedy selection runs in one block
+// (topk_device.cu).  The greedy continues to k2 picks over the same
+// candidates: the first k (T from 2k of the seeds or of `prev`) are the exact
+// greedy picks; all of them are non-overlapping, which is all the next call's
+// threshold needs.  prev may alias picks and prev_n npicks.  *status: 0, or
+// 1 when more windows than the hit list holds fell under T.
+int run_topk_device(cdtw_handle h, const float* x, int64_t N, const double* mu,
+                    const float* sigma, bool euclid, int k, int k2, char* ws_base,
+                    const int32_t* prev, const int* prev_n, int32_t* picks, float* pick_d,
+                    int* npicks, int* status) {
+    const QueryPack& q = h->q;
+    const int M = q.M;
+    const int64_t Nw = N - M + 1;
+    if (k < 1 || k2 < k || (prev && k2 < 2 * k))
+        return set_error(h, CDTW_EINVAL, "device top-k: k=%d, k2=%d", k, k2);
+    SearchWs ws;
+    TopkWs tw;
+    TopkDevWs dw;
+    carve_topk_device(N, M, q.W, k2, &ws, &tw, &dw, ws_base);
+    const int64_t cap = topk_cap(Nw);
+    const int nseg = (int)div_up(Nw, 2 * (int64_t)M);
+    CDTW_CUDA(h, cudaMemsetAsync(ws.ctr, 0, sizeof(int) * 8, h->stream));
+    CDTW_CUDA(h, cudaMemsetAsync(tw.nh, 0, sizeof(int) * 2, h->stream));
+    // 1. LB_Kim of every window, one seed per segment, their exact cDTW
+    CDTW_TRY(launch_lb_kim(h, x, N, mu, sigma, nullptr, Nw, euclid, ws.lbkim));
+    topk_seed_kernel<<<(unsigned)div_up((int64_t)nseg * 32, 256), 256, 0, h->stream>>>(
+        ws.lbkim, (int)Nw, M, nseg, tw.sidx);
+    CDTW_LAUNCH(h, "topk_seed_kernel");
+    CDTW_TRY(launch_cdtw_windows(h, x, N, mu, sigma, tw.sidx, nseg, euclid, tw.sd));
+    // 2. the threshold (the previous windows re-scored with this query)
+    if (prev && prev_n)
+        CDTW_TRY(launch_cdtw_windows(h, x, N, mu, sigma, prev, k2, euclid, dw.prev_d));
+    CDTW_TRY(launch_topk_threshold(h, tw.sd, nseg, dw.prev_d, prev ? prev_n : nullptr, 2 * k,
+                                   ws.key, dw.T));
+    // 3. bounds against T, the survivors' cDTW collected as hits
+    const int grid = h->sm_count * 8;
+    compact_kim_kernel<<<grid, 256, 0, h->stream>>>(ws.lbkim, (int)Nw, ws.key, ws.q1, ws.ctr + 0);
+    CDTW_LAUNCH(h, "compact_kim_kernel");
+    CDTW_TRY(launch_keogh(h, x, N, mu, sigma, euclid, ws));
+    HitSink sink;
+    sink.hits = tw.hits;
+    sink.n = tw.nh;
+    sink.cap = (int)cap;
+    CDTW_TRY(launch_cdtw_search(h, x, N, mu, sigma, ws.q2, ws.ctr + 1, ws.ctr + 3, (int)Nw,
+                                euclid, ws.key, sink));
+    // 4. greedy selection
+    CDTW_CUDA(h, cudaMemsetAsync(dw.acc, 0xff, sizeof(int) * ((size_t)dw.nbuckets + 2),
+                                 h->stream));
+    return launch_topk_greedy(h, tw.hits, tw.nh, (int)cap, k2, M, dw.acc, picks, pick_d, npicks,
+                              status);
+}
+
 size_t search_workspace_bytes(int64_t N, int M, int W) {
     SearchWs ws;
     return carve_search(N, N - M + 1, M, W, &ws, nullptr);

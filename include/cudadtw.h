@@ -152,6 +152,17 @@ int cdtw_topk(cdtw_handle h, const float* d_subject, int64_t N, const double* d_
               const float* d_std, int metric, int k, int64_t* locations, float* distances,
               int* found);
 
+/* cdtw_topk with every step on the device: the threshold by radix selection,
+ * the windows under it collected by the early-abandoning search kernels, the
+ * greedy selection in one thread block (the keys ordered only as far as it
+ * consumes them).  The same picks as cdtw_topk; one host sync at the end.
+ * The steps are those each iteration of cdtw_refine_templates_search runs
+ * inside its CUDA graph.  CDTW_EUNSUPPORTED when more than min(N-M+1, 2^24)
+ * windows fall under the threshold. */
+int cdtw_topk_device(cdtw_handle h, const float* d_subject, int64_t N, const double* d_avg,
+                     const float* d_std, int metric, int k, int64_t* locations,
+                     float* distances, int* found);
+
 /* The whole GPU-DTW search from host buffers (GPU-dtw.cu:59-90): H2D of the
  * subject and query, z-normalisation, statistics, pruned search. */
 int cdtw_search_host(cdtw_handle h, const float* h_query, int M, const float* h_subject,
@@ -393,6 +404,22 @@ int cdtw_pair_bwd(cdtw_handle h, const float* d_q, const float* d_s, int64_t n, 
 int cdtw_refine_templates(cdtw_handle h, const float* d_subject, int64_t N, float* d_templates,
                           const int* Ms, const int* Ws, int nt, const int64_t* locations, int k,
                           int steps, float lr, int metric, float* losses);
+
+/* cdtw_refine_templates with the matches searched again at every step, all
+ * inside the one CUDA graph: each step runs, per template, the device top-k
+ * search of cdtw_topk_device (its candidate threshold also lowered by the
+ * previous step's picks re-scored with the updated template), gathers the k
+ * best non-overlapping windows as the pairs, then the pairwise forward,
+ * backward and Adam update as cdtw_refine_templates.  Step `steps` only
+ * searches and scores.  losses (host, (steps+1) x nt, may be NULL): mean
+ * cDTW of each template to its matches of that step; locations (host,
+ * nt x k, may be NULL): the matches of the last step, best first.  Needs
+ * 11 <= M, W <= CDTW_PAIR_MAX_BAND and at least 2k segments of 2M windows
+ * in the subject for every template (which guarantees k matches). */
+int cdtw_refine_templates_search(cdtw_handle h, const float* d_subject, int64_t N,
+                                 float* d_templates, const int* Ms, const int* Ws, int nt,
+                                 int k, int steps, float lr, int metric, float* losses,
+                                 int64_t* locations);
 
 /* ---- kernel selection ----------------------------------------------------------- */
 

@@ -1,5 +1,7 @@
 """Template refinement (cdtw_refine_templates) through the C ABI: top-k matches
-per template, then Adam steps on the templates, all steps in one graph.
+per template, then Adam steps on the templates, all steps in one graph; and
+the refinement that searches the matches again at every step inside the
+graph (cdtw_refine_templates_search).
 
 * steps = 0: the reported losses are the mean z-normalised cDTW of each
   template over its matches, equal to the FP64 oracle's to 1e-4.
@@ -94,3 +96,56 @@ def test_refine_rejects_bad_windows(setup):
     bad[0, 0] = x.size  # past the end
     with pytest.raises(CudaDTWError):
         h.refine_templates(dx, temps, bands, bad, steps=1)
+
+
+def test_search_refine_zero_steps_matches_topk_and_fp64(setup):
+    """steps = 0: the matches are the top-k of each template, the loss the
+    FP64 oracle's mean distance to them."""
+    h, x, dx, temps, bands, locs = setup
+    new, losses, got = h.refine_templates_search(dx, temps, bands, 20, steps=0)
+    for t, (q, w) in enumerate(zip(temps, bands)):
+        avg, std = h.avg_std(dx, q.size)
+        h.set_query(q, w)
+        want, _ = h.topk(dx, avg, std, 20)
+        np.testing.assert_array_equal(got[t], want)
+    ref, _ = fp64_loss_and_grad(x, temps, bands, got)
+    np.testing.assert_allclose(losses[0], ref, rtol=1e-4)
+    for a, b in zip(new, temps):
+        np.testing.assert_array_equal(a, b)
+
+
+def test_search_refine_first_step_equals_fixed_match_refine(setup):
+    """The first step searches the same matches as cdtw_topk and runs the same
+    kernels on them: one step gives bit-identical templates and losses to
+    the fixed-match refinement given those matches."""
+    h, x, dx, temps, bands, locs = setup
+    a, la, _ = h.refine_templates_search(dx, temps, bands, 20, steps=1, lr=1e-2)
+    b, lb = h.refine_templates(dx, temps, bands, locs, steps=1, lr=1e-2)
+    np.testing.assert_array_equal(la[0], lb[0])
+    for u, v in zip(a, b):
+        np.testing.assert_array_equal(u, v)
+
+
+def test_search_refine_many_steps(setup):
+    """30 steps with fresh matches at every step: the last step's matches are
+    the top-k of the refined templates (host top-k search), the last loss row
+    equals the FP64 recheck against them, and the mean loss falls."""
+    h, x, dx, temps, bands, locs = setup
+    new, losses, got = h.refine_templates_search(dx, temps, bands, 20, steps=30, lr=1e-2)
+    assert losses.shape == (31, len(temps))
+    for t, (q, w) in enumerate(zip(new, bands)):
+        avg, std = h.avg_std(dx, q.size)
+        h.set_query(q, w)
+        want, _ = h.topk(dx, avg, std, 20)
+        np.testing.assert_array_equal(got[t], want)
+    ref, _ = fp64_loss_and_grad(x, new, bands, got)
+    np.testing.assert_allclose(losses[-1], ref, rtol=1e-4)
+    assert losses[-1].mean() < losses[0].mean()
+
+
+def test_search_refine_rejects_short_subject(setup):
+    from cudadtw_b200 import CudaDTWError
+    h, x, dx, temps, bands, locs = setup
+    with pytest.raises(CudaDTWError):
+        # 2^16 samples hold 512 segments of 2 x 64 windows: fewer than 2k
+        h.refine_templates_search(dx, temps[:1], bands[:1], 300, steps=1)

@@ -60,6 +60,33 @@ def test_topk_equals_greedy_over_all_windows(handle, kind, n, M, P, k, metric):
     assert np.all(np.diff(np.sort(locs)) >= M)
 
 
+@pytest.mark.parametrize("kind,n,M,P,k,metric", [
+    ("ecg", 1 << 16, 64, 10, 20, 0),
+    ("ecg", 1 << 16, 128, 20, 50, 1),
+    ("metal", 1 << 17, 96, 5, 200, 0),
+    ("walk", 1 << 16, 200, 10, 40, 0),    # random walk: dense candidate valleys
+    ("ecg", 1 << 18, 64, 10, 1000, 0),    # several ordered key blocks in the greedy
+    ("ecg", 4000, 64, 10, 1000, 0),       # fewer non-overlapping windows than k
+])
+def test_topk_device_equals_host_topk(handle, kind, n, M, P, k, metric):
+    """cdtw_topk_device (threshold, collection and greedy selection on the
+    device) returns exactly cdtw_topk's picks and distances."""
+    x = {"ecg": lambda: synth.ecg_like(n, seed=7), "metal": lambda: synth.metal_like(n, seed=8),
+         "walk": lambda: synth.random_walk(n, 9)}[kind]()
+    q, _ = synth.cut_query(x, M, seed=9, noise=0.05)
+    W = synth.band_from_percent(M, P)
+    dx = torch.from_numpy(x).cuda()
+    avg, std = handle.avg_std(dx, M)
+    handle.set_query(q, W)
+    hl, hd = handle.topk(dx, avg, std, k, metric=metric)
+    dl, dd = handle.topk_device(dx, avg, std, k, metric=metric)
+    np.testing.assert_array_equal(dl, hl)
+    np.testing.assert_array_equal(dd, hd)
+    if n > 4000:
+        full = handle.gpu_cdtw(dx, avg, std, metric=metric).cpu().numpy()
+        np.testing.assert_array_equal(dl, greedy(full, k, M))
+
+
 def test_topk_errors(handle):
     from cudadtw_b200 import CudaDTWError
     x = torch.from_numpy(synth.ecg_like(5000, seed=1)).cuda()
