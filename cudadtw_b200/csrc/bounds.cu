@@ -195,7 +195,88 @@ lb_keogh_kernel(const float* __restrict__ x, const double* __restrict__ mu,
     if (rev) rev[t] = ar;
 }
 
+// Front part of LB_Kim of every window (the search's first pass; the back
+// part is added only for the windows the front part does not prune, see
+// kim_back_compact_kernel), and per block of kKimSeedBlock windows the one of
+// smallest front bound as a seed.  A warp takes one such block, a lane eight
+// consecutive windows: their front samples are twelve consecutive stream
+// values and the five query values stay in registers.
+constexpr int kKimSeedBlock = 256;
+constexpr int kFrontPerLane = kKimSeedBlock / 32;
+
+template <bool EU>
+__global__ void __launch_bounds__(256)
+lb_kim_front_kernel(const float* __restrict__ x, int64_t N, const double* __restrict__ mu,
+                    const float* __restrict__ sigma, const float* __restrict__ zq, int Nw,
+                    float* __restrict__ front, unsigned long long* __restrict__ seeds) {
+    float q[5];
+#pragma unroll
+    for (int k = 0; k < 5; ++k) q[k] = __ldg(zq + k);
+    const int lane = threadIdx.x & 31;
+    const int64_t nblk = ((int64_t)Nw + kKimSeedBlock - 1) / kKimSeedBlock;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t b = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; b < nblk;
+         b += nwarps) {
+        const int64_t w0 = b * kKimSeedBlock + (int64_t)lane * kFrontPerLane;
+        unsigned long long best = ~0ull;
+        if (w0 < Nw) {
+            float xv[kFrontPerLane + 4];
+#pragma unroll
+            for (int j = 0; j < kFrontPerLane + 4; ++j)
+                xv[j] = (w0 + j < N) ? __ldg(x + w0 + j) : 0.f;
+            float f[kFrontPerLane];
+#pragma unroll
+            for (int i = 0; i < kFrontPerLane; ++i) {
+                const int64_t w = w0 + i;
+                f[i] = CDTW_INF;
+                if (w < Nw) {
+                    const Norm nm = make_norm(__ldg(mu + w), __ldg(sigma + w));
+                    float sv[5];
+#pragma unroll
+                    for (int k = 0; k < 5; ++k) sv[k] = znorm(nm, xv[i + k]);
+                    f[i] = lb_kim_front<EU>(sv, q);
+                    if (f[i] == f[i]) best = min(best, pack_key(f[i], (uint32_t)w));
+                }
+            }
+            if (w0 + kFrontPerLane <= Nw) {  // front is 256-byte aligned, w0 a multiple of 8
+                float4* o = reinterpret_cast<float4*>(front + w0);
+                o[0] = make_float4(f[0], f[1], f[2], f[3]);
+                o[1] = make_float4(f[4], f[5], f[6], f[7]);
+            } else {
+#pragma unroll
+                for (int i = 0; i < kFrontPerLane; ++i)
+                    if (w0 + i < Nw) front[w0 + i] = f[i];
+            }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) best = min(best, __shfl_xor_sync(0xffffffffu, best, o));
+        if (lane == 0) seeds[b] = best;
+    }
+}
+
 }  // namespace
+
+int launch_lb_kim_front(cdtw_handle h, const float* x, int64_t N, const double* mu,
+                        const float* sigma, bool euclid, float* front,
+                        unsigned long long* seeds) {
+    const QueryPack& q = h->q;
+    if (q.M < 11)
+        return set_error(h, CDTW_EINVAL,
+                         "LB_Kim is a 10-point DTW: the query needs at least 11 samples");
+    const int64_t Nw = N - q.M + 1;
+    if (Nw <= 0) return CDTW_OK;
+    const int64_t warps = div_up(Nw, kKimSeedBlock);
+    const unsigned blocks =
+        (unsigned)std::max<int64_t>(1, std::min<int64_t>(div_up(warps, 8), (int64_t)h->sm_count * 8));
+    if (euclid)
+        lb_kim_front_kernel<true><<<blocks, 256, 0, h->stream>>>(x, N, mu, sigma, q.zq, (int)Nw,
+                                                                  front, seeds);
+    else
+        lb_kim_front_kernel<false><<<blocks, 256, 0, h->stream>>>(x, N, mu, sigma, q.zq, (int)Nw,
+                                                                   front, seeds);
+    CDTW_LAUNCH(h, "lb_kim_front_kernel");
+    return CDTW_OK;
+}
 
 int launch_lb_kim(cdtw_handle h, const float* x, int64_t N, const double* mu, const float* sigma,
                   const int32_t* idx, int64_t L, bool euclid, float* out,

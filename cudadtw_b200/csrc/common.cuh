@@ -208,9 +208,10 @@ __device__ __forceinline__ float znorm(const Norm& n, float x) {
 // s[0..4] (front) / s[5..9] (back) and the matching query values q[0..9]:
 // 5x5 unconstrained DTW at the front (min over its last row and column) plus
 // the 5x5 back block entered anywhere on its first row/column, the
-// recurrences of include/bounds.cuh:315-404.
+// recurrences of include/bounds.cuh:315-404.  The two parts are independent:
+// lb_kim_front + lb_kim_back, added in that order, is the bound.
 template <bool EU>
-__device__ __forceinline__ float lb_kim_dp(const float (&s)[10], const float (&q)[10]) {
+__device__ __forceinline__ float lb_kim_front(const float* s, const float* q) {
     auto lp = [](float d) { return EU ? d * d : fabsf(d); };
     float F[5], G[5];
     F[0] = lp(q[0] - s[0]);
@@ -228,18 +229,30 @@ __device__ __forceinline__ float lb_kim_dp(const float (&s)[10], const float (&q
     }
 #pragma unroll
     for (int k = 0; k < 4; ++k) mem = fminf(mem, F[k]);
+    return mem;
+}
+
+// s / q: the last five window samples / query values.
+template <bool EU>
+__device__ __forceinline__ float lb_kim_back(const float* s, const float* q) {
+    auto lp = [](float d) { return EU ? d * d : fabsf(d); };
+    float F[5], G[5];
 #pragma unroll
-    for (int k = 0; k < 5; ++k) F[k] = lp(q[5] - s[5 + k]);
+    for (int k = 0; k < 5; ++k) F[k] = lp(q[0] - s[k]);
 #pragma unroll
     for (int r = 1; r < 5; ++r) {
-        G[0] = lp(q[5 + r] - s[5]);
+        G[0] = lp(q[r] - s[0]);
 #pragma unroll
-        for (int k = 1; k < 5; ++k)
-            G[k] = lp(q[5 + r] - s[5 + k]) + min3f(G[k - 1], F[k - 1], F[k]);
+        for (int k = 1; k < 5; ++k) G[k] = lp(q[r] - s[k]) + min3f(G[k - 1], F[k - 1], F[k]);
 #pragma unroll
         for (int k = 0; k < 5; ++k) F[k] = G[k];
     }
-    return mem + F[4];
+    return F[4];
+}
+
+template <bool EU>
+__device__ __forceinline__ float lb_kim_dp(const float (&s)[10], const float (&q)[10]) {
+    return lb_kim_front<EU>(s, q) + lb_kim_back<EU>(s + 5, q + 5);
 }
 
 // Packed (distance, index) key for the fused argmin: distances are >= 0 so
@@ -390,6 +403,11 @@ int max_register_band();
 int launch_lb_kim(cdtw_handle h, const float* x, int64_t N, const double* mu, const float* sigma,
                   const int32_t* idx, int64_t L, bool euclid, float* out,
                   unsigned long long* seeds = nullptr, unsigned* bmax = nullptr);
+// The search's first pass: the front part of LB_Kim of every window into
+// front (256-byte aligned), the smallest per 256 windows into seeds.
+int launch_lb_kim_front(cdtw_handle h, const float* x, int64_t N, const double* mu,
+                        const float* sigma, bool euclid, float* front,
+                        unsigned long long* seeds);
 size_t stream_envelope_scratch_bytes(int64_t N);
 // gate: when set, the kernel does nothing if *gate <= gate_max (a device
 // count the host cannot see, e.g. the LB_Kim survivors of a search).
