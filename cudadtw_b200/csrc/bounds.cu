@@ -195,70 +195,87 @@ lb_keogh_kernel(const float* __restrict__ x, const double* __restrict__ mu,
     if (rev) rev[t] = ar;
 }
 
-// Front part of LB_Kim of every window (the search's first pass; the back
-// part is added only for the windows the front part does not prune, see
-// kim_back_compact_kernel), and per block of kKimSeedBlock windows the one of
-// smallest front bound as a seed.  A warp takes one such block, a lane eight
-// consecutive windows: their front samples are twelve consecutive stream
-// values and the five query values stay in registers.
+// LB_Kim of every window for the search's first pass, with per block of
+// kKimSeedBlock windows the one of smallest bound (a seed) and the largest
+// bound.  A warp takes one such block, a lane eight consecutive windows:
+// their front samples are twelve consecutive stream values, their back
+// samples another twelve, and the ten query values stay in registers (the
+// same arithmetic as lb_kim_kernel, window by window).
 constexpr int kKimSeedBlock = 256;
-constexpr int kFrontPerLane = kKimSeedBlock / 32;
+constexpr int kKimPerLane = kKimSeedBlock / 32;
 
 template <bool EU>
 __global__ void __launch_bounds__(256)
-lb_kim_front_kernel(const float* __restrict__ x, int64_t N, const double* __restrict__ mu,
-                    const float* __restrict__ sigma, const float* __restrict__ zq, int Nw,
-                    float* __restrict__ front, unsigned long long* __restrict__ seeds) {
-    float q[5];
+lb_kim_all_kernel(const float* __restrict__ x, int64_t N, const double* __restrict__ mu,
+                  const float* __restrict__ sigma, const float* __restrict__ zq, int M, int Nw,
+                  float* __restrict__ out, unsigned long long* __restrict__ seeds,
+                  unsigned* __restrict__ bmax) {
+    float qf[5], qb[5];
 #pragma unroll
-    for (int k = 0; k < 5; ++k) q[k] = __ldg(zq + k);
+    for (int k = 0; k < 5; ++k) {
+        qf[k] = __ldg(zq + k);
+        qb[k] = __ldg(zq + M - 5 + k);
+    }
     const int lane = threadIdx.x & 31;
     const int64_t nblk = ((int64_t)Nw + kKimSeedBlock - 1) / kKimSeedBlock;
     const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
     for (int64_t b = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; b < nblk;
          b += nwarps) {
-        const int64_t w0 = b * kKimSeedBlock + (int64_t)lane * kFrontPerLane;
+        const int64_t w0 = b * kKimSeedBlock + (int64_t)lane * kKimPerLane;
         unsigned long long best = ~0ull;
+        unsigned mx = 0u;
         if (w0 < Nw) {
-            float xv[kFrontPerLane + 4];
+            float xf[kKimPerLane + 4], xb[kKimPerLane + 4];
 #pragma unroll
-            for (int j = 0; j < kFrontPerLane + 4; ++j)
-                xv[j] = (w0 + j < N) ? __ldg(x + w0 + j) : 0.f;
-            float f[kFrontPerLane];
+            for (int j = 0; j < kKimPerLane + 4; ++j) {
+                xf[j] = (w0 + j < N) ? __ldg(x + w0 + j) : 0.f;
+                xb[j] = (w0 + M - 5 + j < N) ? __ldg(x + w0 + M - 5 + j) : 0.f;
+            }
+            float f[kKimPerLane];
 #pragma unroll
-            for (int i = 0; i < kFrontPerLane; ++i) {
+            for (int i = 0; i < kKimPerLane; ++i) {
                 const int64_t w = w0 + i;
                 f[i] = CDTW_INF;
                 if (w < Nw) {
                     const Norm nm = make_norm(__ldg(mu + w), __ldg(sigma + w));
-                    float sv[5];
+                    float sf[5], sb[5];
 #pragma unroll
-                    for (int k = 0; k < 5; ++k) sv[k] = znorm(nm, xv[i + k]);
-                    f[i] = lb_kim_front<EU>(sv, q);
-                    if (f[i] == f[i]) best = min(best, pack_key(f[i], (uint32_t)w));
+                    for (int k = 0; k < 5; ++k) {
+                        sf[k] = znorm(nm, xf[i + k]);
+                        sb[k] = znorm(nm, xb[i + k]);
+                    }
+                    f[i] = lb_kim_front<EU>(sf, qf) + lb_kim_back<EU>(sb, qb);
+                    if (f[i] == f[i]) {
+                        best = min(best, pack_key(f[i], (uint32_t)w));
+                        mx = max(mx, __float_as_uint(f[i]));
+                    }
                 }
             }
-            if (w0 + kFrontPerLane <= Nw) {  // front is 256-byte aligned, w0 a multiple of 8
-                float4* o = reinterpret_cast<float4*>(front + w0);
+            if (w0 + kKimPerLane <= Nw) {  // out is 256-byte aligned, w0 a multiple of 8
+                float4* o = reinterpret_cast<float4*>(out + w0);
                 o[0] = make_float4(f[0], f[1], f[2], f[3]);
                 o[1] = make_float4(f[4], f[5], f[6], f[7]);
             } else {
 #pragma unroll
-                for (int i = 0; i < kFrontPerLane; ++i)
-                    if (w0 + i < Nw) front[w0 + i] = f[i];
+                for (int i = 0; i < kKimPerLane; ++i)
+                    if (w0 + i < Nw) out[w0 + i] = f[i];
             }
         }
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) best = min(best, __shfl_xor_sync(0xffffffffu, best, o));
-        if (lane == 0) seeds[b] = best;
+        mx = __reduce_max_sync(0xffffffffu, mx);
+        if (lane == 0) {
+            seeds[b] = best;
+            bmax[b] = mx;
+        }
     }
 }
 
 }  // namespace
 
-int launch_lb_kim_front(cdtw_handle h, const float* x, int64_t N, const double* mu,
-                        const float* sigma, bool euclid, float* front,
-                        unsigned long long* seeds) {
+int launch_lb_kim_all(cdtw_handle h, const float* x, int64_t N, const double* mu,
+                      const float* sigma, bool euclid, float* out, unsigned long long* seeds,
+                      unsigned* bmax) {
     const QueryPack& q = h->q;
     if (q.M < 11)
         return set_error(h, CDTW_EINVAL,
@@ -266,15 +283,15 @@ int launch_lb_kim_front(cdtw_handle h, const float* x, int64_t N, const double* 
     const int64_t Nw = N - q.M + 1;
     if (Nw <= 0) return CDTW_OK;
     const int64_t warps = div_up(Nw, kKimSeedBlock);
-    const unsigned blocks =
-        (unsigned)std::max<int64_t>(1, std::min<int64_t>(div_up(warps, 8), (int64_t)h->sm_count * 8));
+    const unsigned blocks = (unsigned)std::max<int64_t>(
+        1, std::min<int64_t>(div_up(warps, 8), (int64_t)h->sm_count * 8));
     if (euclid)
-        lb_kim_front_kernel<true><<<blocks, 256, 0, h->stream>>>(x, N, mu, sigma, q.zq, (int)Nw,
-                                                                  front, seeds);
+        lb_kim_all_kernel<true><<<blocks, 256, 0, h->stream>>>(x, N, mu, sigma, q.zq, q.M,
+                                                                (int)Nw, out, seeds, bmax);
     else
-        lb_kim_front_kernel<false><<<blocks, 256, 0, h->stream>>>(x, N, mu, sigma, q.zq, (int)Nw,
-                                                                   front, seeds);
-    CDTW_LAUNCH(h, "lb_kim_front_kernel");
+        lb_kim_all_kernel<false><<<blocks, 256, 0, h->stream>>>(x, N, mu, sigma, q.zq, q.M,
+                                                                 (int)Nw, out, seeds, bmax);
+    CDTW_LAUNCH(h, "lb_kim_all_kernel");
     return CDTW_OK;
 }
 

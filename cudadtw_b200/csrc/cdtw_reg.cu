@@ -31,6 +31,8 @@ struct RegKernels {
     RegKernel mh2[kMaxReg2W + 1];
     RegKernel eu4[kMaxReg4W + 1];  // four windows per thread
     RegKernel mh4[kMaxReg4W + 1];
+    RegCKernel euc[kMaxReg2W + 1];  // consecutive windows, all of them
+    RegCKernel mhc[kMaxReg2W + 1];
     RegKernels() {
         void** a = (void**)eu;
         void** b = (void**)mh;
@@ -45,6 +47,9 @@ struct RegKernels {
         reg2_fill_part0((void**)eu2, (void**)mh2);
         reg2_fill_part1((void**)eu2, (void**)mh2);
         reg4_fill_part0((void**)eu4, (void**)mh4);
+        regc_fill_part0((void**)euc, (void**)mhc);
+        regc_fill_part1((void**)euc, (void**)mhc);
+        regc_fill_part2((void**)euc, (void**)mhc);
     }
 };
 
@@ -126,11 +131,25 @@ int launch_cdtw_windows(cdtw_handle h, const float* x, int64_t N, const double* 
     // four windows per thread up to W = kMaxReg4W, two up to kMaxReg2W
     // (register budget)
     const int per = q.W <= kMaxReg4W ? 4 : (q.W <= kMaxReg2W ? 2 : 1);
+    const int lq4 = q.lq / 4;
+    const size_t smem = (size_t)q.lq * 4 * sizeof(float);
+    if (!idx && per > 1 && L == Nw) {
+        // every window: the consecutive-window kernels (one sliding run of
+        // the stream per thread)
+        RegCKernel kc = euclid ? reg_kernels().euc[q.W] : reg_kernels().mhc[q.W];
+        if (smem > 48 * 1024)
+            CDTW_CUDA(h, cudaFuncSetAttribute((const void*)kc,
+                                              cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                              (int)smem));
+        const unsigned blocks = (unsigned)div_up(div_up(L, per), kRegBlock);
+        kc<<<blocks, kRegBlock, smem, h->stream>>>(x, mu, sigma, (const float4*)q.qpad, lq4, q.M,
+                                                   Nw, out);
+        CDTW_LAUNCH(h, "cdtw_regc_kernel");
+        return CDTW_OK;
+    }
     RegKernel k = per == 4   ? (euclid ? reg_kernels().eu4[q.W] : reg_kernels().mh4[q.W])
                   : per == 2 ? (euclid ? reg_kernels().eu2[q.W] : reg_kernels().mh2[q.W])
                              : (euclid ? reg_kernels().eu[q.W] : reg_kernels().mh[q.W]);
-    const int lq4 = q.lq / 4;
-    const size_t smem = (size_t)q.lq * 4 * sizeof(float);
     if (smem > 48 * 1024)
         CDTW_CUDA(h, cudaFuncSetAttribute((const void*)k,
                                           cudaFuncAttributeMaxDynamicSharedMemorySize,

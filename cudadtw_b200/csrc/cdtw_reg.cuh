@@ -246,6 +246,127 @@ cdtw_reg4_kernel(const float* __restrict__ x, const double* __restrict__ mu,
         if (4 * t + v < L) out[4 * t + v] = ok[v] ? r[v] : __int_as_float(0x7fc00000);
 }
 
+// All windows, NW consecutive ones per thread (windows NW t .. NW t + NW - 1,
+// no index list): window v's sample at row j is x[NW t + v + j], so the NW
+// windows of a thread read one sliding run of the stream.  Rows go in groups
+// of four; a group needs NW + 3 consecutive samples, of which four are new:
+// they are loaded one group ahead and the run is shifted by four at the end
+// of the group.  Every group but the last runs without row-index clamps or
+// result tests; the last (one to four rows) ends at row M - 1.
+template <int W, bool EU, int NW>
+__device__ __forceinline__ void regc_row(float (&p)[NW][2 * W + 2], const float (&z)[NW],
+                                         const float4* qr) {
+    constexpr int B = 2 * W + 1;
+    constexpr int NQ4 = (B + 3) / 4;
+    float qv[NQ4 * 4];
+#pragma unroll
+    for (int r = 0; r < NQ4; ++r) {
+        const float4 a = qr[r];
+        qv[4 * r + 0] = a.x;
+        qv[4 * r + 1] = a.y;
+        qv[4 * r + 2] = a.z;
+        qv[4 * r + 3] = a.w;
+    }
+    float l[NW];
+#pragma unroll
+    for (int v = 0; v < NW; ++v) l[v] = CDTW_INF;
+#pragma unroll
+    for (int k = 0; k < B; ++k) {
+#pragma unroll
+        for (int v = 0; v < NW; ++v) {
+            const float m = min3f(p[v][k], p[v][k + 1], l[v]);
+            l[v] = cell<EU>(z[v] - qv[k], m);
+            p[v][k] = l[v];  // p[v][k] is not read again this row
+        }
+    }
+}
+
+template <int W, bool EU, int NW>
+__global__ void __launch_bounds__(kRegBlock, 1)
+cdtw_regc_kernel(const float* __restrict__ x, const double* __restrict__ mu,
+                 const float* __restrict__ sigma, const float4* __restrict__ qpad4, int lq4,
+                 int M, int Nw, float* __restrict__ out) {
+    extern __shared__ float4 sq4[];
+    for (int e = threadIdx.x; e < 4 * lq4; e += blockDim.x) sq4[e] = qpad4[e];
+    __syncthreads();
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int w0 = t * NW;
+    if (w0 >= Nw) return;
+    constexpr int B = 2 * W + 1;
+    constexpr int NX = NW + 3;  // samples of a group of four rows
+    // the last thread's missing windows repeat window Nw - 1's statistics and
+    // read clamped samples; they are not stored
+    const int rem = Nw - 1 - w0;                 // windows after w0 (>= 0)
+    const int xlast = rem + M - 1;               // last sample index from w0
+    const float* __restrict__ xb = x + w0;
+    Norm nm[NW];
+#pragma unroll
+    for (int v = 0; v < NW; ++v) {
+        const int w = w0 + min(v, rem);
+        nm[v] = make_norm(mu[w], sigma[w]);
+    }
+    float p[NW][B + 1];
+#pragma unroll
+    for (int v = 0; v < NW; ++v) {
+#pragma unroll
+        for (int k = 0; k <= B; ++k) p[v][k] = CDTW_INF;
+        p[v][W] = 0.0f;
+    }
+    float xs[NX];
+#pragma unroll
+    for (int i = 0; i < NX; ++i) xs[i] = __ldg(xb + min(i, xlast));
+    int j0 = 0;
+    for (; j0 + 4 < M; j0 += 4) {
+        float nx[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) nx[i] = __ldg(xb + min(j0 + NX + i, xlast));
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            float z[NW];
+#pragma unroll
+            for (int v = 0; v < NW; ++v) z[v] = znorm(nm[v], xs[u + v]);
+            regc_row<W, EU, NW>(p, z, sq4 + u * lq4 + (j0 >> 2));
+        }
+#pragma unroll
+        for (int i = 0; i + 4 < NX; ++i) xs[i] = xs[i + 4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) xs[NX - 4 + i] = nx[i];
+    }
+    float r[NW];
+#pragma unroll
+    for (int v = 0; v < NW; ++v) r[v] = CDTW_INF;
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+        if (j0 + u < M) {
+            float z[NW];
+#pragma unroll
+            for (int v = 0; v < NW; ++v) z[v] = znorm(nm[v], xs[u + v]);
+            regc_row<W, EU, NW>(p, z, sq4 + u * lq4 + (j0 >> 2));
+            if (j0 + u == M - 1) {
+#pragma unroll
+                for (int v = 0; v < NW; ++v) r[v] = p[v][W];
+            }
+        }
+    }
+#pragma unroll
+    for (int v = 0; v < NW; ++v)
+        if (v <= rem) out[w0 + v] = r[v];
+}
+
+using RegCKernel = void (*)(const float*, const double*, const float*, const float4*, int, int,
+                            int, float*);
+
+template <int LO, int HI, int NW>
+struct RegCRange {
+    static void fill(RegCKernel* eu, RegCKernel* mh) {
+        if constexpr (LO <= HI) {
+            eu[LO] = cdtw_regc_kernel<LO, true, NW>;
+            mh[LO] = cdtw_regc_kernel<LO, false, NW>;
+            RegCRange<LO + 1, HI, NW>::fill(eu, mh);
+        }
+    }
+};
+
 // cDTW of one window (xw, normalisation nm) against the query whose padded
 // copies sit in shared memory (sq4, lq4 float4 per copy) with its envelope
 // senv, abandoning once the last row minimum plus the remaining suffix of the
@@ -422,5 +543,10 @@ void reg_fill_part5(void** eu, void** mh, void** seu, void** smh);
 void reg2_fill_part0(void** eu, void** mh);  // two-window kernels, cdtw_reg2_part*.cu
 void reg2_fill_part1(void** eu, void** mh);
 void reg4_fill_part0(void** eu, void** mh);  // four-window kernels, cdtw_reg4_part0.cu
+// all-windows kernels over consecutive windows (cdtw_regc_part*.cu): four per
+// thread for W <= kMaxReg4W, two for W <= kMaxReg2W
+void regc_fill_part0(void** eu, void** mh);
+void regc_fill_part1(void** eu, void** mh);
+void regc_fill_part2(void** eu, void** mh);
 
 }  // namespace cdtw

@@ -209,7 +209,10 @@ __device__ __forceinline__ float znorm(const Norm& n, float x) {
 // 5x5 unconstrained DTW at the front (min over its last row and column) plus
 // the 5x5 back block entered anywhere on its first row/column, the
 // recurrences of include/bounds.cuh:315-404.  The two parts are independent:
-// lb_kim_front + lb_kim_back, added in that order, is the bound.
+// lb_kim_front + lb_kim_back, added in that order, is the bound.  (Seeding
+// the search from the front part alone, the back part computed only where
+// the front part passes, was measured: its seeds are poor enough that the
+// first best-so-far prunes almost nothing on some queries.)
 template <bool EU>
 __device__ __forceinline__ float lb_kim_front(const float* s, const float* q) {
     auto lp = [](float d) { return EU ? d * d : fabsf(d); };
@@ -403,11 +406,11 @@ int max_register_band();
 int launch_lb_kim(cdtw_handle h, const float* x, int64_t N, const double* mu, const float* sigma,
                   const int32_t* idx, int64_t L, bool euclid, float* out,
                   unsigned long long* seeds = nullptr, unsigned* bmax = nullptr);
-// The search's first pass: the front part of LB_Kim of every window into
-// front (256-byte aligned), the smallest per 256 windows into seeds.
-int launch_lb_kim_front(cdtw_handle h, const float* x, int64_t N, const double* mu,
-                        const float* sigma, bool euclid, float* front,
-                        unsigned long long* seeds);
+// The search's first pass: LB_Kim of every window into out (256-byte
+// aligned), per 256 windows the smallest (seeds) and the largest (bmax).
+int launch_lb_kim_all(cdtw_handle h, const float* x, int64_t N, const double* mu,
+                      const float* sigma, bool euclid, float* out, unsigned long long* seeds,
+                      unsigned* bmax);
 size_t stream_envelope_scratch_bytes(int64_t N);
 // gate: when set, the kernel does nothing if *gate <= gate_max (a device
 // count the host cannot see, e.g. the LB_Kim survivors of a search).

@@ -35,7 +35,6 @@ namespace cdtw {
 constexpr int kPairThreads = 128;
 constexpr int kWalkChunk = 64;  // bytes of direction record per lane in one backtracking chunk
 constexpr unsigned kFull = 0xffffffffu;
-constexpr int kPrefetch = 4;  // edge-lane series values loaded ahead
 
 struct PairArgs {
     const float* zq;      // DP inputs: n x L (z-normalised copies or the raw series);
@@ -122,30 +121,8 @@ struct PairLane {
     float A[C], B[C], Q[C], Sv[C], lim[C];
     uint32_t bits;  // direction bits of the last anti-diagonal
     int iq, js;    // lane 0's slot-0 query index, lane G-1's last-slot subject index
-    // the edge lanes' next values: pq[d] at iq + 1 + d, ps[d] at js + 1 + d
-    // (loaded kPrefetch shifts, 2 kPrefetch anti-diagonals, before their use)
-    float pq[kPrefetch], ps[kPrefetch];
+    float pq, ps;  // the values at iq + 1 / js + 1 (the next shift's)
 };
-
-// The edge lanes' prefetch queues from the current iq / js.
-template <int C>
-__device__ __forceinline__ void prefetch_init(PairLane<C>& st, const float* sq, const float* ss,
-                                              int L) {
-#pragma unroll
-    for (int d = 0; d < kPrefetch; ++d) {
-        st.pq[d] = (st.iq + 1 + d < L) ? __ldg(sq + st.iq + 1 + d) : 0.f;
-        st.ps[d] = (st.js + 1 + d < L) ? __ldg(ss + st.js + 1 + d) : 0.f;
-    }
-}
-
-// Advance a queue by one value: q[0] is consumed, the value at idx + kPrefetch
-// (idx: the index just consumed) is loaded into the last slot.
-__device__ __forceinline__ void prefetch_pop(float (&q)[kPrefetch], const float* src, int idx,
-                                             int L) {
-#pragma unroll
-    for (int d = 0; d + 1 < kPrefetch; ++d) q[d] = q[d + 1];
-    q[kPrefetch - 1] = (idx + kPrefetch < L) ? __ldg(src + idx + kPrefetch) : 0.f;
-}
 
 // Direction element of anti-diagonal k: to the pair's global record (DM 1,
 // live groups only) or to the group's shared-memory record (DM 2).
@@ -166,10 +143,10 @@ __device__ __forceinline__ void step_odd(PairLane<C>& st, const float* ss, int L
     if (shift) {
         constexpr int slot = (RS - 1 + C) % C;
         const float v = __shfl_down_sync(kFull, st.Sv[slot], 1, G);
-        st.Sv[slot] = (l == G - 1) ? st.ps[0] : v;
+        st.Sv[slot] = (l == G - 1) ? st.ps : v;
         if (l == G - 1) {
             ++st.js;
-            prefetch_pop(st.ps, ss, st.js, L);
+            st.ps = st.js + 1 < L ? __ldg(ss + st.js + 1) : 0.f;
         }
     }
     float nb = __shfl_down_sync(kFull, st.A[0], 1, G);
@@ -183,10 +160,10 @@ __device__ __forceinline__ void step_even(PairLane<C>& st, const float* sq, int 
     if (shift) {
         constexpr int slot = (C - RQ) % C;  // = (C - 1 - (RQ - 1)) mod C
         const float v = __shfl_up_sync(kFull, st.Q[slot], 1, G);
-        st.Q[slot] = (l == 0) ? st.pq[0] : v;
+        st.Q[slot] = (l == 0) ? st.pq : v;
         if (l == 0) {
             ++st.iq;
-            prefetch_pop(st.pq, sq, st.iq, L);
+            st.pq = st.iq + 1 < L ? __ldg(sq + st.iq + 1) : 0.f;
         }
     }
     float nb = __shfl_up_sync(kFull, st.B[C - 1], 1, G);
@@ -428,7 +405,8 @@ __device__ __forceinline__ int pair_begin(PairLane<C>& st, const float* sq, cons
     st.bits = 0;
     st.iq = (W - e0) / 2;                      // lane 0's slot-0 query index at k = 0
     st.js = (-W + 2 * (G * C - 1) + e0) / 2;  // lane G-1's last-slot subject index
-    prefetch_init(st, sq, ss, L);
+    st.pq = (st.iq + 1 < L) ? __ldg(sq + st.iq + 1) : 0.f;
+    st.ps = (st.js + 1 < L) ? __ldg(ss + st.js + 1) : 0.f;
     int k = 0;
     if (e0 == 0) {
         step_even<C, EU, DIRS, 0, 0>(st, sq, L, G, l, false);
@@ -443,10 +421,10 @@ __device__ __forceinline__ int pair_begin(PairLane<C>& st, const float* sq, cons
             const float v = __shfl_up_sync(kFull, st.Q[C - 1], 1, G);
 #pragma unroll
             for (int c = C - 1; c > 0; --c) st.Q[c] = st.Q[c - 1];
-            st.Q[0] = (l == 0) ? st.pq[0] : v;
+            st.Q[0] = (l == 0) ? st.pq : v;
             if (l == 0) {
                 ++st.iq;
-                prefetch_pop(st.pq, sq, st.iq, L);
+                st.pq = st.iq + 1 < L ? __ldg(sq + st.iq + 1) : 0.f;
             }
             step_even<C, EU, DIRS, 0, 0>(st, sq, L, G, l, false);
             store_dirs<C, DM>(st, drow, G, l, k, live);
@@ -494,7 +472,8 @@ __device__ __forceinline__ void ckpt_restore(PairLane<C>& st, const float* ck, c
     st.bits = 0;
     st.iq = (km + W - em) / 2;                            // lane 0, slot 0 at k-1
     st.js = (km - W + 2 * (G * C - 1) + em) / 2;          // lane G-1, last slot at k-1
-    prefetch_init(st, sq, ss, L);
+    st.pq = (st.iq + 1 < L) ? __ldg(sq + st.iq + 1) : 0.f;
+    st.ps = (st.js + 1 < L) ? __ldg(ss + st.js + 1) : 0.f;
 }
 
 // DM: 0 distance only; 1 path record in global scratch, walked through a

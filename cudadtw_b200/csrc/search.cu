@@ -189,89 +189,6 @@ compact_kim_kernel(const float* __restrict__ lbkim, int Nw, const unsigned long 
     }
 }
 
-// The search's LB_Kim compaction from the front parts alone: a window whose
-// front part already fails the bound is pruned without the rest; the others
-// get the back part (lb_kim_back on their last five samples) added, the same
-// sum as the whole-window LB_Kim, and are kept when that passes.  Survivors'
-// full bounds go to lbkim (which holds the front parts on entry).  *kmax:
-// the largest LB_Kim of all windows (float bits) when none is pruned, else
-// +inf bits: a pruned window's bound exceeds the best-so-far, and so the
-// final best, which is all the termination flag (best < largest LB_Kim)
-// needs.
-template <bool EU>
-__global__ void __launch_bounds__(256)
-kim_back_compact_kernel(const float* __restrict__ x, const double* __restrict__ mu,
-                        const float* __restrict__ sigma, const float* __restrict__ zq, int M,
-                        int Nw, float* __restrict__ lbkim, const unsigned long long* key,
-                        int* __restrict__ q1, int* __restrict__ n1, unsigned* __restrict__ kmax) {
-    const float bsf = load_bsf(key);
-    float qb[5];
-#pragma unroll
-    for (int k = 0; k < 5; ++k) qb[k] = __ldg(zq + M - 5 + k);
-    const int lane = threadIdx.x & 31;
-    const int nvec = (Nw + 3) >> 2;
-    const int stride = gridDim.x * blockDim.x;
-    bool pruned = false;
-    unsigned mx = 0u;
-    for (int base = (blockIdx.x * blockDim.x + threadIdx.x) & ~31; base < nvec; base += stride) {
-        const int v = base + lane;
-        const int64_t w0 = 4 * (int64_t)v;
-        float fv[4] = {CDTW_INF, CDTW_INF, CDTW_INF, CDTW_INF};
-        if (w0 + 3 < Nw) {
-            const float4 f = __ldcs(reinterpret_cast<const float4*>(lbkim) + v);
-            fv[0] = f.x;
-            fv[1] = f.y;
-            fv[2] = f.z;
-            fv[3] = f.w;
-        } else {
-#pragma unroll
-            for (int j = 0; j < 4; ++j)
-                if (w0 + j < Nw) fv[j] = lbkim[w0 + j];
-        }
-        unsigned keep = 0u;
-#pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            const int64_t w = w0 + j;
-            const bool in = w < Nw;
-            const bool cand = in && fv[j] * kLbSlack < bsf;
-            pruned = pruned || (in && !cand);
-            if (!__any_sync(0xffffffffu, cand)) continue;
-            if (cand) {
-                const Norm nm = make_norm(mu[w], sigma[w]);
-                float sv[5];
-#pragma unroll
-                for (int k = 0; k < 5; ++k) sv[k] = znorm(nm, __ldg(x + w + M - 5 + k));
-                const float full = fv[j] + lb_kim_back<EU>(sv, qb);
-                if (full * kLbSlack < bsf) {
-                    keep |= 1u << j;
-                    lbkim[w] = full;
-                    mx = max(mx, __float_as_uint(full));
-                } else {
-                    pruned = true;
-                }
-            }
-        }
-        const int c = __popc(keep);
-        int pre = c;  // inclusive prefix over the lanes
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const int t = __shfl_up_sync(0xffffffffu, pre, o);
-            if (lane >= o) pre += t;
-        }
-        const int tot = __shfl_sync(0xffffffffu, pre, 31);
-        if (!tot) continue;
-        int at = 0;
-        if (lane == 31) at = atomicAdd(n1, tot);
-        at = __shfl_sync(0xffffffffu, at, 31) + pre - c;
-#pragma unroll
-        for (int j = 0; j < 4; ++j)
-            if (keep & (1u << j)) q1[at++] = (int)w0 + j;
-    }
-    const bool any_pruned = __any_sync(0xffffffffu, pruned);
-    mx = __reduce_max_sync(0xffffffffu, mx);
-    if (lane == 0) atomicMax(kmax, any_pruned ? __float_as_uint(CDTW_INF) : mx);
-}
-
 // Forward + reverse LB_Keogh of the compacted windows; survivors -> q2.
 template <bool EU>
 __global__ void __launch_bounds__(256)
@@ -810,15 +727,14 @@ int run_search(cdtw_handle h, const float* x, int64_t N, const double* mu, const
     } else {
         CDTW_CUDA(h, cudaMemsetAsync(ws.key, 0xff, sizeof(unsigned long long), h->stream));
     }
-    // 1. front part of LB_Kim of every window + per-block seeds (the back
-    //    part only for the windows the front part leaves, at the compaction)
+    // 1. LB_Kim of every window + per-block seeds
     const int64_t nblk = div_up(Nw, kKimBlock);
-    CDTW_TRY(launch_lb_kim_front(h, x, N, mu, sigma, euclid, ws.lbkim, ws.seeds));
+    CDTW_TRY(launch_lb_kim_all(h, x, N, mu, sigma, euclid, ws.lbkim, ws.seeds, ws.bmax));
     // 2. cDTW of the seeds
     const int G = (int)std::max<int64_t>(1, div_up(nblk, seed_target(q.M, q.W)));
     const int nseed = (int)div_up(nblk, G);
     seeds_to_cands_kernel<<<(unsigned)div_up(nseed, 256), 256, 0, h->stream>>>(
-        ws.seeds, nullptr, (int)nblk, G, ws.seed_cands, ws.ctr + 4, (unsigned*)ws.ctr + 5);
+        ws.seeds, ws.bmax, (int)nblk, G, ws.seed_cands, ws.ctr + 4, (unsigned*)ws.ctr + 5);
     CDTW_LAUNCH(h, "seeds_to_cands_kernel");
     // the seeds only bound the search from above, so their cDTW runs as
     // pairwise wavefronts (a lane group per seed: low latency with few
@@ -840,15 +756,8 @@ int run_search(cdtw_handle h, const float* x, int64_t N, const double* mu, const
     }
     // 3. compaction by LB_Kim
     const int grid = h->sm_count * 8;
-    if (euclid)
-        kim_back_compact_kernel<true><<<grid, 256, 0, h->stream>>>(
-            x, mu, sigma, q.zq, q.M, (int)Nw, ws.lbkim, ws.key, ws.q1, ws.ctr + 0,
-            (unsigned*)ws.ctr + 5);
-    else
-        kim_back_compact_kernel<false><<<grid, 256, 0, h->stream>>>(
-            x, mu, sigma, q.zq, q.M, (int)Nw, ws.lbkim, ws.key, ws.q1, ws.ctr + 0,
-            (unsigned*)ws.ctr + 5);
-    CDTW_LAUNCH(h, "kim_back_compact_kernel");
+    compact_kim_kernel<<<grid, 256, 0, h->stream>>>(ws.lbkim, (int)Nw, ws.key, ws.q1, ws.ctr + 0);
+    CDTW_LAUNCH(h, "compact_kim_kernel");
     // 4. LB_Keogh forward + reverse
     CDTW_TRY(launch_keogh(h, x, N, mu, sigma, euclid, ws));
     // 5. cDTW of the survivors: as pairwise wavefronts when at most `wcap`
