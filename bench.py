@@ -450,11 +450,16 @@ def subresults(h, dev) -> dict:
     ws = [b[1] for b in batch]
     h.search_batched(dx, qs, ws)
     tb, (bl, bd) = dev_time(lambda: h.search_batched(dx, qs, ws))
-    tp, pres = dev_time(plain)
+    counts = []
+    tp, pres = dev_time(lambda: plain(counts))
     same = sum(int(a == r[0]) for a, r in zip(bl, pres))
+    short_cells = sum(float(c[2]) * cells(q.size, w) for q, w, c in zip(qs, ws, counts))
     out["batched_search_short"] = {"queries": len(qs), "stream": "ecg 2^20", "M": [64, 128],
                                    "batched_s": tb, "plain_s": tp, "speedup": tp / tb,
-                                   "same_location": same}
+                                   "same_location": same,
+                                   "plain_cdtw_windows": int(sum(c[2] for c in counts[:len(qs)])),
+                                   "plain_cdtw_cells": short_cells,
+                                   "cell_floor_s_at_7800_gcups": short_cells / 7.8e12}
     del dx
 
     # -- search over a stream pushed in pieces (host buffers) ---------------

@@ -62,6 +62,11 @@ const RegKernels& reg_kernels() {
 
 int max_register_band() { return kMaxRegW; }
 
+bool lane_eligible(cdtw_handle h) {
+    int G, B;
+    return lane_shape(h->q.W, &G, &B) && h->q.lq >= lane_qpad_min(h->q.M, h->q.W);
+}
+
 int choose_variant(cdtw_handle h, int W) {
     int v = (W >= 0 && W < CDTW_MAX_QUERY) ? h->band_variant[W] : 0;
     int G, B;
@@ -141,7 +146,8 @@ int launch_cdtw_windows(cdtw_handle h, const float* x, int64_t N, const double* 
             CDTW_CUDA(h, cudaFuncSetAttribute((const void*)kc,
                                               cudaFuncAttributeMaxDynamicSharedMemorySize,
                                               (int)smem));
-        const unsigned blocks = (unsigned)div_up(div_up(L, per), kRegBlock);
+        const unsigned blocks =
+            (unsigned)div_up(div_up(L, regc_per_thread(q.W)), kRegBlock);
         kc<<<blocks, kRegBlock, smem, h->stream>>>(x, mu, sigma, (const float4*)q.qpad, lq4, q.M,
                                                    Nw, out);
         CDTW_LAUNCH(h, "cdtw_regc_kernel");

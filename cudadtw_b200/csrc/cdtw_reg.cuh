@@ -356,6 +356,13 @@ cdtw_regc_kernel(const float* __restrict__ x, const double* __restrict__ mu,
 using RegCKernel = void (*)(const float*, const double*, const float*, const float4*, int, int,
                             int, float*);
 
+// Windows per thread of the consecutive-window kernels (register budget: the
+// three-window kernel spills from W = 32).
+constexpr int kMaxReg3W = 31;
+constexpr int regc_per_thread(int W) {
+    return W <= kMaxReg4W ? 4 : (W <= kMaxReg3W ? 3 : 2);
+}
+
 template <int LO, int HI, int NW>
 struct RegCRange {
     static void fill(RegCKernel* eu, RegCKernel* mh) {
@@ -543,8 +550,8 @@ void reg_fill_part5(void** eu, void** mh, void** seu, void** smh);
 void reg2_fill_part0(void** eu, void** mh);  // two-window kernels, cdtw_reg2_part*.cu
 void reg2_fill_part1(void** eu, void** mh);
 void reg4_fill_part0(void** eu, void** mh);  // four-window kernels, cdtw_reg4_part0.cu
-// all-windows kernels over consecutive windows (cdtw_regc_part*.cu): four per
-// thread for W <= kMaxReg4W, two for W <= kMaxReg2W
+// all-windows kernels over consecutive windows (cdtw_regc_part*.cu), windows
+// per thread regc_per_thread(W)
 void regc_fill_part0(void** eu, void** mh);
 void regc_fill_part1(void** eu, void** mh);
 void regc_fill_part2(void** eu, void** mh);

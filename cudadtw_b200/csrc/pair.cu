@@ -306,17 +306,6 @@ int launch_pair_fwd(cdtw_handle h, const float* zq, const float* zs, int64_t n, 
     int G, C;
     pair_shape(L, W, &G, &C);
     if (C > 16) return set_error(h, CDTW_EUNSUPPORTED, "pair band W=%d exceeds 511", W);
-    if (!rows) {
-        // distance only (no path record whose layout fixes the shape): with
-        // few pairs, wider lane groups of fewer cells give each SM more
-        // warps to hide the per-step latency of the wavefront (the cells are
-        // the same, so D is the same)
-        const int64_t want = (int64_t)16 * h->sm_count;
-        while (G < 32 && C > 1 && n * G / 32 < want) {
-            G *= 2;
-            C = (W + 1 + G - 1) / G;
-        }
-    }
     PairArgs a;
     a.zq = zq;
     a.zs = zs;

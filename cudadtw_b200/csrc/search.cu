@@ -114,6 +114,17 @@ __global__ void wave_keys_kernel(const float* __restrict__ d, const Cand* __rest
 // distance as the search kernels compute it lies below this bound (also for
 // an exact match, distance 0): the bound prunes nothing that could be the
 // best, and the best window replaces it in the key.
+// The same raising for seeds whose cDTW the search kernels computed into a
+// key of their own (skey: the best seed's packed distance and window).
+__global__ void seed_key_bound_kernel(const unsigned long long* __restrict__ skey, int M,
+                                      unsigned long long* __restrict__ key) {
+    const unsigned long long k = *skey;
+    if (k == ~0ull) return;
+    const float d = key_dist(k);
+    if (!(d < CDTW_INF)) return;
+    atomicMin(key, pack_key(d * kSeedBoundSlack + 1e-6f * (float)M, 0xffffffffu));
+}
+
 __global__ void seed_bound_kernel(const float* __restrict__ d, const Cand* __restrict__ cands,
                                   int nseed, int M, unsigned long long* __restrict__ key) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -431,7 +442,7 @@ size_t carve_search(int64_t N, int64_t Nw, int M, int W, SearchWs* ws, char* bas
     ws->xenv = (float2*)take(sizeof(float2) * N);
     ws->envscratch = (float*)take(stream_envelope_scratch_bytes(N));
     ws->ctr = (int*)take(sizeof(int) * 8);
-    ws->key = (unsigned long long*)take(sizeof(unsigned long long));
+    ws->key = (unsigned long long*)take(2 * sizeof(unsigned long long));  // [1]: seeds
     // rows of the seed windows (at most one per LB_Kim block, kSeedMax) and,
     // when that pass can run for this (M, W), of the survivors run as
     // wavefronts (at most kWaveSurvivors)
@@ -721,12 +732,10 @@ int run_search(cdtw_handle h, const float* x, int64_t N, const double* mu, const
     SearchWs ws;
     carve_search(N, Nw, q.M, q.W, &ws, ws_base);
     CDTW_CUDA(h, cudaMemsetAsync(ws.ctr, 0, sizeof(int) * 8, h->stream));
-    if (init_key) {
+    CDTW_CUDA(h, cudaMemsetAsync(ws.key, 0xff, 2 * sizeof(unsigned long long), h->stream));
+    if (init_key)
         CDTW_CUDA(h, cudaMemcpyAsync(ws.key, init_key, sizeof(unsigned long long),
                                      cudaMemcpyDeviceToDevice, h->stream));
-    } else {
-        CDTW_CUDA(h, cudaMemsetAsync(ws.key, 0xff, sizeof(unsigned long long), h->stream));
-    }
     // 1. LB_Kim of every window + per-block seeds
     const int64_t nblk = div_up(Nw, kKimBlock);
     CDTW_TRY(launch_lb_kim_all(h, x, N, mu, sigma, euclid, ws.lbkim, ws.seeds, ws.bmax));
@@ -736,12 +745,20 @@ int run_search(cdtw_handle h, const float* x, int64_t N, const double* mu, const
     seeds_to_cands_kernel<<<(unsigned)div_up(nseed, 256), 256, 0, h->stream>>>(
         ws.seeds, ws.bmax, (int)nblk, G, ws.seed_cands, ws.ctr + 4, (unsigned*)ws.ctr + 5);
     CDTW_LAUNCH(h, "seeds_to_cands_kernel");
-    // the seeds only bound the search from above, so their cDTW runs as
-    // pairwise wavefronts (a lane group per seed: low latency with few
-    // windows in flight) when the band and the seed windows fit
+    // the seeds only bound the search from above (raised a little, with no
+    // window): with few windows in flight their cDTW is latency-bound, so it
+    // runs on the lane-group kernel (band over lanes, rows pipelined) when the
+    // band suits it, else as pairwise wavefronts when the band and the seed
+    // windows fit, else on the search kernels
     const int Wp = std::min(q.W, q.M - 1);
-    if (Wp <= CDTW_PAIR_MAX_BAND && q.M <= CDTW_MAX_QUERY && nseed <= kSeedMax &&
-        (int64_t)nseed * q.M <= ws.seed_cap) {
+    const bool lane = lane_eligible(h);
+    if (lane) {
+        CDTW_TRY(launch_cdtw_lane_search(h, x, N, mu, sigma, ws.seed_cands, ws.ctr + 4,
+                                         ws.ctr + 2, nseed, euclid, ws.key + 1, HitSink()));
+        seed_key_bound_kernel<<<1, 1, 0, h->stream>>>(ws.key + 1, q.M, ws.key);
+        CDTW_LAUNCH(h, "seed_key_bound_kernel");
+    } else if (Wp <= CDTW_PAIR_MAX_BAND && q.M <= CDTW_MAX_QUERY && nseed <= kSeedMax &&
+               (int64_t)nseed * q.M <= ws.seed_cap) {
         seed_gather_kernel<<<(unsigned)div_up((int64_t)nseed * 32, 256), 256, 0, h->stream>>>(
             x, mu, sigma, ws.seed_cands, nseed, q.M, ws.seed_z);
         CDTW_LAUNCH(h, "seed_gather_kernel");
@@ -752,7 +769,9 @@ int run_search(cdtw_handle h, const float* x, int64_t N, const double* mu, const
         CDTW_LAUNCH(h, "seed_bound_kernel");
     } else {
         CDTW_TRY(launch_cdtw_search(h, x, N, mu, sigma, ws.seed_cands, ws.ctr + 4, ws.ctr + 2,
-                                    nseed, euclid, ws.key));
+                                    nseed, euclid, ws.key + 1));
+        seed_key_bound_kernel<<<1, 1, 0, h->stream>>>(ws.key + 1, q.M, ws.key);
+        CDTW_LAUNCH(h, "seed_key_bound_kernel");
     }
     // 3. compaction by LB_Kim
     const int grid = h->sm_count * 8;
@@ -760,11 +779,19 @@ int run_search(cdtw_handle h, const float* x, int64_t N, const double* mu, const
     CDTW_LAUNCH(h, "compact_kim_kernel");
     // 4. LB_Keogh forward + reverse
     CDTW_TRY(launch_keogh(h, x, N, mu, sigma, euclid, ws));
-    // 5. cDTW of the survivors: as pairwise wavefronts when at most `wcap`
-    //    remain and a window is long enough that a thread per window is
-    //    latency-bound, else with early abandoning
+    // 5. cDTW of the survivors: when at most kWaveSurvivors remain and a
+    //    window is long enough that a thread per window is latency-bound, on
+    //    the lane-group kernel (or as pairwise wavefronts where the band does
+    //    not suit it; at most `wcap`), else on the search kernel of the band;
+    //    the gated launch does nothing above its limit and otherwise takes
+    //    every candidate from the shared work counter, so the next launch
+    //    finds none left
     const int wcap = (int)std::min<int64_t>(kWaveSurvivors, ws.seed_cap / q.M);
-    if (wave_eligible(q.M, q.W) && wcap >= 32) {
+    if (wave_eligible(q.M, q.W) && lane) {
+        CDTW_TRY(launch_cdtw_lane_search(h, x, N, mu, sigma, ws.q2, ws.ctr + 1, ws.ctr + 3,
+                                         kWaveSurvivors, euclid, ws.key, HitSink(),
+                                         kWaveSurvivors));
+    } else if (wave_eligible(q.M, q.W) && wcap >= 32) {
         wave_gather_kernel<<<(unsigned)div_up((int64_t)wcap * 32, 256), 256, 0, h->stream>>>(
             x, mu, sigma, ws.q2, ws.ctr + 1, wcap, q.M, ws.seed_z, ws.ctr + 3);
         CDTW_LAUNCH(h, "wave_gather_kernel");
