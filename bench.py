@@ -286,22 +286,23 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
                         "h2d_bytes_per_step": len(bands) * (x.nbytes + q.nbytes),
                         "d2h_bytes_per_step": len(bands) * nw * 4},
                 "roofline": {"bound": "alu",
-                             "kernel": "cdtw_reg4_kernel (W=12) + cdtw_reg2_kernel (W=25)",
+                             "kernel": "cdtw_regc_kernel<12,EU,4> (W=12) + "
+                                       "cdtw_regc_kernel<25,EU,3> (W=25)",
                              "achieved": ach, "peak": peak / 1e9, "unit": "GCUPS",
                              "frac": ach / (peak / 1e9),
-                             # DRAM bytes (read + write) of one cdtw_reg2_kernel launch
-                             # of this workload from an ncu capture (both bands 69.2 MB:
+                             # DRAM bytes (read + write) of one launch of this workload
+                             # from an ncu capture (70.2 / 70.0 MB for W = 12 / 25:
                              # stream, window statistics, results); not measured here
-                             "traffic": 69.2e6, "traffic_unit": "bytes per launch",
+                             "traffic": 70.1e6, "traffic_unit": "bytes per launch",
                              "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write"
-                                               ".sum, profiles/cdtw_reg2_kernel_raw_allwindows"
+                                               ".sum, profiles/cdtw_regc_kernel_raw_allwindows"
                                                "_m128_n4M.md",
                              "per_band": {str(w): a for w, a in zip(bands, achieved)},
                              "peak_source": "measured: cdtw_calibrate_cell_rate (FADD+FMNMX3+FFMA"
                                             " chains) on this GPU in this run"},
                 "argmin": {str(w): b for w, b in zip(bands, best)}, "cut_offset": off}
         if world == 1 and not args.no_sub:
-            line["subresults"] = subresults(h, dev)
+            line["subresults"] = subresults(h, dev, peak)
         if world == 1:
             g, thr, n, dt = cpu_port_gcups(x, q, bands, 10.0)
             line["cpu_baseline"] = {
@@ -312,7 +313,7 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
     h.close()
 
 
-def subresults(h, dev) -> dict:
+def subresults(h, dev, peak=None) -> dict:
     """The other scope rows, measured beside the headline (one GPU, rank 0).
 
     * pruned_search: config 0 (2^20 ECG-like, M=128, W=12) and config 1
@@ -329,6 +330,8 @@ def subresults(h, dev) -> dict:
     * pair_fwd_bwd: config 3 (4096 pairs, L=256, W=25, z-normalised random
       walks) and its L=2048/W=409 variant: forward (D only), forward with the
       path record, backward, and their ratio; CUDA-graph replays, device time.
+    * wide_band_all_windows: all-windows cDTW of 2^18 windows at M=1024 for
+      W = 102, 204, 409 (the lane-group kernel).
     """
     import torch
     from cudadtw_b200 import synth
@@ -540,6 +543,22 @@ def subresults(h, dev) -> dict:
         pair[f"{n}x{L}_W{W}"] = r
         del q, s, path, gq, gs
     out["pair_fwd_bwd"] = pair
+
+    # -- wide bands: the lane-group kernel, all windows -----------------------
+    x = synth.metal_like((1 << 18) + 1023, seed=1)
+    dx = torch.from_numpy(x).to(dev)
+    q, _ = synth.cut_query(x, 1024, seed=5, noise=0.1)
+    avg, std = h.avg_std(dx, 1024)
+    wide = {}
+    for W in (102, 204, 409):
+        h.set_query(q, W)
+        h.gpu_cdtw(dx, avg, std)  # warm-up
+        t, _ = dev_time(lambda: h.gpu_cdtw(dx, avg, std), reps=3)
+        g = (1 << 18) * cells(1024, W) / t / 1e9
+        wide[f"W{W}"] = {"ms": t * 1e3, "gcups": g, "variant": "lane group",
+                         "frac_of_measured_cell_rate": g / (peak / 1e9) if peak else None}
+    out["wide_band_all_windows"] = {"stream": "metal 2^18 windows", "M": 1024, "bands": wide}
+    del dx
     out["refine"] = refine_subresult(h, dev)
     return out
 

@@ -118,7 +118,7 @@ int launch_cdtw_lane(cdtw_handle h, const float* x, int64_t N, const double* mu,
 int launch_cdtw_lane_search(cdtw_handle h, const float* x, int64_t N, const double* mu,
                             const float* sigma, const Cand* cands, const int* count, int* work,
                             int max_count, bool euclid, unsigned long long* key,
-                            const HitSink& sink, int gate_max) {
+                            const HitSink& sink) {
     if (max_count <= 0) return CDTW_OK;
     LaneArgs a;
     CDTW_TRY(fill_lane_args(h, x, N, mu, sigma, &a));
@@ -129,7 +129,6 @@ int launch_cdtw_lane_search(cdtw_handle h, const float* x, int64_t N, const doub
     a.work = work;
     a.key = key;
     a.sink = sink;
-    a.gate_max = gate_max;
     const LaneKernel k = euclid ? lane_kernels().seu[B] : lane_kernels().smh[B];
     const size_t smem = lane_smem(h->q);
     CDTW_CUDA(h, cudaFuncSetAttribute((const void*)k, cudaFuncAttributeMaxDynamicSharedMemorySize,

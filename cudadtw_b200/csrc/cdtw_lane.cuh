@@ -63,7 +63,6 @@ struct LaneArgs {
     int* work;
     unsigned long long* key;
     HitSink sink;
-    int gate_max = -1;    // >= 0: the search does nothing when *count exceeds it
 };
 
 constexpr int kLaneThreads = 256;
@@ -325,7 +324,6 @@ cdtw_lane_search_kernel(const LaneArgs a) {
     const int h = lane >> a.lgG;  // group in warp
     const int per_warp = 64 >> a.lgG;
     const int n = *(const volatile int*)a.count;
-    if (a.gate_max >= 0 && n > a.gate_max) return;  // uniform for the whole launch
     for (;;) {
         int base = 0;
         if (lane == 0) base = atomicAdd(a.work, per_warp);

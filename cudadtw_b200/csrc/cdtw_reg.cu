@@ -62,11 +62,6 @@ const RegKernels& reg_kernels() {
 
 int max_register_band() { return kMaxRegW; }
 
-bool lane_eligible(cdtw_handle h) {
-    int G, B;
-    return lane_shape(h->q.W, &G, &B) && h->q.lq >= lane_qpad_min(h->q.M, h->q.W);
-}
-
 int choose_variant(cdtw_handle h, int W) {
     int v = (W >= 0 && W < CDTW_MAX_QUERY) ? h->band_variant[W] : 0;
     int G, B;

@@ -394,10 +394,7 @@ int launch_cdtw_lane(cdtw_handle h, const float* x, int64_t N, const double* mu,
 int launch_cdtw_lane_search(cdtw_handle h, const float* x, int64_t N, const double* mu,
                             const float* sigma, const Cand* cands, const int* count, int* work,
                             int max_count, bool euclid, unsigned long long* key,
-                            const HitSink& sink, int gate_max = -1);
-// lane-group kernels serve this handle's query band (27 <= W <= 767 and a
-// query pack long enough)
-bool lane_eligible(cdtw_handle h);
+                            const HitSink& sink);
 // floats per shifted query copy (QueryPack::lq) of a handle's query pack
 inline int qpad_len(int M, int W) { return (int)(((int64_t)M + 2 * W + 56 + 3) / 4 * 4); }
 // Kernel choice for band W: CDTW_VARIANT_REGISTER (one thread per window, band

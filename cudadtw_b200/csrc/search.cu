@@ -747,18 +747,14 @@ int run_search(cdtw_handle h, const float* x, int64_t N, const double* mu, const
     CDTW_LAUNCH(h, "seeds_to_cands_kernel");
     // the seeds only bound the search from above (raised a little, with no
     // window): with few windows in flight their cDTW is latency-bound, so it
-    // runs on the lane-group kernel (band over lanes, rows pipelined) when the
-    // band suits it, else as pairwise wavefronts when the band and the seed
-    // windows fit, else on the search kernels
+    // runs as pairwise wavefronts (a lane group per seed) when the band and
+    // the seed windows fit, else on the search kernels (into a key of their
+    // own, raised the same way).  The lane-group search kernel was measured
+    // slower here than the wavefronts (M=512, W=51: 1.04 against 0.66 ms per
+    // search).
     const int Wp = std::min(q.W, q.M - 1);
-    const bool lane = lane_eligible(h);
-    if (lane) {
-        CDTW_TRY(launch_cdtw_lane_search(h, x, N, mu, sigma, ws.seed_cands, ws.ctr + 4,
-                                         ws.ctr + 2, nseed, euclid, ws.key + 1, HitSink()));
-        seed_key_bound_kernel<<<1, 1, 0, h->stream>>>(ws.key + 1, q.M, ws.key);
-        CDTW_LAUNCH(h, "seed_key_bound_kernel");
-    } else if (Wp <= CDTW_PAIR_MAX_BAND && q.M <= CDTW_MAX_QUERY && nseed <= kSeedMax &&
-               (int64_t)nseed * q.M <= ws.seed_cap) {
+    if (Wp <= CDTW_PAIR_MAX_BAND && q.M <= CDTW_MAX_QUERY && nseed <= kSeedMax &&
+        (int64_t)nseed * q.M <= ws.seed_cap) {
         seed_gather_kernel<<<(unsigned)div_up((int64_t)nseed * 32, 256), 256, 0, h->stream>>>(
             x, mu, sigma, ws.seed_cands, nseed, q.M, ws.seed_z);
         CDTW_LAUNCH(h, "seed_gather_kernel");
@@ -779,19 +775,11 @@ int run_search(cdtw_handle h, const float* x, int64_t N, const double* mu, const
     CDTW_LAUNCH(h, "compact_kim_kernel");
     // 4. LB_Keogh forward + reverse
     CDTW_TRY(launch_keogh(h, x, N, mu, sigma, euclid, ws));
-    // 5. cDTW of the survivors: when at most kWaveSurvivors remain and a
-    //    window is long enough that a thread per window is latency-bound, on
-    //    the lane-group kernel (or as pairwise wavefronts where the band does
-    //    not suit it; at most `wcap`), else on the search kernel of the band;
-    //    the gated launch does nothing above its limit and otherwise takes
-    //    every candidate from the shared work counter, so the next launch
-    //    finds none left
+    // 5. cDTW of the survivors: as pairwise wavefronts when at most `wcap`
+    //    remain and a window is long enough that a thread per window is
+    //    latency-bound, else with early abandoning
     const int wcap = (int)std::min<int64_t>(kWaveSurvivors, ws.seed_cap / q.M);
-    if (wave_eligible(q.M, q.W) && lane) {
-        CDTW_TRY(launch_cdtw_lane_search(h, x, N, mu, sigma, ws.q2, ws.ctr + 1, ws.ctr + 3,
-                                         kWaveSurvivors, euclid, ws.key, HitSink(),
-                                         kWaveSurvivors));
-    } else if (wave_eligible(q.M, q.W) && wcap >= 32) {
+    if (wave_eligible(q.M, q.W) && wcap >= 32) {
         wave_gather_kernel<<<(unsigned)div_up((int64_t)wcap * 32, 256), 256, 0, h->stream>>>(
             x, mu, sigma, ws.q2, ws.ctr + 1, wcap, q.M, ws.seed_z, ws.ctr + 3);
         CDTW_LAUNCH(h, "wave_gather_kernel");
