@@ -252,9 +252,7 @@ cdtw_reg4_kernel(const float* __restrict__ x, const double* __restrict__ mu,
 // of four; a group needs NW + 3 consecutive samples, of which four are new:
 // they are loaded one group ahead and the run is shifted by four at the end
 // of the group.  Every group but the last runs without row-index clamps or
-// result tests; the last (one to four rows) ends at row M - 1.  Groups in the
-// first and last W rows compute only the chunks of four band cells that lie
-// inside the matrix (regc_row_clipped).
+// result tests; the last (one to four rows) ends at row M - 1.
 template <int W, bool EU, int NW>
 __device__ __forceinline__ void regc_row(float (&p)[NW][2 * W + 2], const float (&z)[NW],
                                          const float4* qr) {
@@ -279,41 +277,6 @@ __device__ __forceinline__ void regc_row(float (&p)[NW][2 * W + 2], const float 
             const float m = min3f(p[v][k], p[v][k + 1], l[v]);
             l[v] = cell<EU>(z[v] - qv[k], m);
             p[v][k] = l[v];  // p[v][k] is not read again this row
-        }
-    }
-}
-
-// A row of the band's first or last W rows, where the cells outside the
-// matrix (query position < 0 or >= M) are +inf whatever is computed: only the
-// chunks of four cells kc_lo .. kc_hi (warp-uniform) are computed.  The cells
-// skipped before the range were never computed (they stay +inf); those after
-// it are never read by a cell inside the matrix (a cell reads the cells above
-// and above-right at the same or a smaller query position), so stale values
-// there do no harm.
-template <int W, bool EU, int NW>
-__device__ __forceinline__ void regc_row_clipped(float (&p)[NW][2 * W + 2], const float (&z)[NW],
-                                                 const float4* qr, int kc_lo, int kc_hi) {
-    constexpr int B = 2 * W + 1;
-    constexpr int NQ4 = (B + 3) / 4;
-    float l[NW];
-#pragma unroll
-    for (int v = 0; v < NW; ++v) l[v] = CDTW_INF;
-#pragma unroll
-    for (int r = 0; r < NQ4; ++r) {
-        if (r < kc_lo || r > kc_hi) continue;
-        const float4 a = qr[r];
-        const float qv[4] = {a.x, a.y, a.z, a.w};
-#pragma unroll
-        for (int kk = 0; kk < 4; ++kk) {
-            const int k = 4 * r + kk;
-            if (k < B) {
-#pragma unroll
-                for (int v = 0; v < NW; ++v) {
-                    const float m = min3f(p[v][k], p[v][k + 1], l[v]);
-                    l[v] = cell<EU>(z[v] - qv[kk], m);
-                    p[v][k] = l[v];
-                }
-            }
         }
     }
 }
@@ -357,25 +320,12 @@ cdtw_regc_kernel(const float* __restrict__ x, const double* __restrict__ mu,
         float nx[4];
 #pragma unroll
         for (int i = 0; i < 4; ++i) nx[i] = __ldg(xb + min(j0 + NX + i, xlast));
-        // band cells inside the matrix somewhere in rows j0 .. j0+3
-        const int k_lo = max(0, W - (j0 + 3)), k_hi = min(B - 1, W + M - 1 - j0);
-        if (k_lo > 0 || k_hi < B - 1) {
 #pragma unroll
-            for (int u = 0; u < 4; ++u) {
-                float z[NW];
+        for (int u = 0; u < 4; ++u) {
+            float z[NW];
 #pragma unroll
-                for (int v = 0; v < NW; ++v) z[v] = znorm(nm[v], xs[u + v]);
-                regc_row_clipped<W, EU, NW>(p, z, sq4 + u * lq4 + (j0 >> 2), k_lo >> 2,
-                                            k_hi >> 2);
-            }
-        } else {
-#pragma unroll
-            for (int u = 0; u < 4; ++u) {
-                float z[NW];
-#pragma unroll
-                for (int v = 0; v < NW; ++v) z[v] = znorm(nm[v], xs[u + v]);
-                regc_row<W, EU, NW>(p, z, sq4 + u * lq4 + (j0 >> 2));
-            }
+            for (int v = 0; v < NW; ++v) z[v] = znorm(nm[v], xs[u + v]);
+            regc_row<W, EU, NW>(p, z, sq4 + u * lq4 + (j0 >> 2));
         }
 #pragma unroll
         for (int i = 0; i + 4 < NX; ++i) xs[i] = xs[i + 4];
