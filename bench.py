@@ -643,7 +643,7 @@ def profile_case(name: str) -> None:
     """One small run of a scope row (twice, untimed) for an ncu capture:
     search = config-1 pruned search (2^25 metal-like, M=512, P=10); strip /
     wide = all-windows cDTW of 2^18 windows at M=1024, W=204 (strip kernel /
-    lane-group kernel);
+    lane-group kernel), wide409 the same at W=409 (lane-group kernel);
     batch_short = the batched search of 512 queries (M 64-128) on a 2^20 ECG-like
     stream; topk =
     top-1000 of one M=256 template on a 2^22 ECG-like stream; pair = 256 pairs
@@ -675,15 +675,17 @@ def profile_case(name: str) -> None:
                 dx = torch.from_numpy(x).to(dev)
                 batch = synth.batch_queries(x, 512, seed=3, m_lo=64, m_hi=128)
                 h.search_batched(dx, [b[0] for b in batch], [b[1] for b in batch])
-            elif name in ("strip", "wide"):
-                # all-windows cDTW of 2^18 windows at M=1024, W=204: the strip
-                # kernel ("strip") or the lane-group kernel ("wide")
+            elif name in ("strip", "wide", "wide409"):
+                # all-windows cDTW of 2^18 windows at M=1024, W=204 (W=409 for
+                # "wide409"): the strip kernel ("strip") or the lane-group
+                # kernel
+                W = 409 if name == "wide409" else 204
                 x = synth.metal_like((1 << 18) + 1023, seed=1)
                 dx = torch.from_numpy(x).to(dev)
                 q, _ = synth.cut_query(x, 1024, seed=5, noise=0.1)
                 avg, std = h.avg_std(dx, 1024)
-                h.set_query(q, 204)
-                h.set_band_variant(204, 204, "strip16" if name == "strip" else "lane")
+                h.set_query(q, W)
+                h.set_band_variant(W, W, "strip16" if name == "strip" else "lane")
                 h.gpu_cdtw(dx, avg, std)
             elif name == "pair":
                 for n, L, W in ((256, 2048, 409), (4096, 256, 25)):
@@ -739,7 +741,7 @@ def main() -> None:
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--profile",
                     choices=["search", "topk", "pair", "refine", "refine_search", "strip", "wide",
-                             "batch_short"],
+                             "wide409", "batch_short"],
                     help="run one small case of that row twice (for ncu) and exit")
     ap.add_argument("--no-sub", action="store_true",
                     help="skip the pruned / batched search and pair fwd/bwd sub-results")
