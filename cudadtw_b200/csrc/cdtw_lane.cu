@@ -5,6 +5,7 @@
 #include "cdtw_lane.cuh"
 
 #include <algorithm>
+#include <mutex>
 
 namespace cdtw {
 
@@ -28,8 +29,68 @@ const LaneKernels& lane_kernels() {
     return k;
 }
 
-// Shared-memory floats of the query copies the kernels stage per block.
-size_t lane_smem(const QueryPack& q) { return (size_t)4 * q.lq * sizeof(float); }
+// Float4s between the starts of consecutive query copies in shared memory
+// (the copy rounded up to 8 float4s, plus 8 for the bank offsets below).
+int lane_copy_stride(const QueryPack& q) { return (q.lq / 4 + 7) / 8 * 8 + 8; }
+
+// Shared-memory bytes of the query copies the kernels stage per block.
+size_t lane_smem(const QueryPack& q) {
+    return (size_t)4 * lane_copy_stride(q) * sizeof(float4);
+}
+
+// Bank offsets of the query copies.  At step t lane g of a group reads the
+// float4s b >> 2, (b >> 2) + 1, ... of copy b & 3, b = t + g (B-1).  Eight
+// lanes' 16-byte reads (a quarter warp) are served in one shared-memory
+// wavefront when their float4 indices differ mod 8, so copy c is placed at
+// c * stride + e[c] (stride a multiple of 8) with e[c] in [0, 8) chosen to
+// minimise the wavefronts of the reads over the 32-step period of the
+// pattern (the groups of a warp read the same addresses; e[0] = 0).  With the
+// copies back to back the reads of a wide band took up to 11 wavefronts per
+// instruction against 4 at best.
+void lane_copy_offsets(int B, int G, int e[4]) {
+    static std::mutex mu;
+    static bool done[kLaneBMax + 1][6] = {};
+    static int table[kLaneBMax + 1][6][4];
+    int lg = 0;
+    while ((1 << lg) < G) ++lg;
+    std::lock_guard<std::mutex> lock(mu);
+    if (!done[B][lg]) {
+        const int D = B - 1;
+        long best = -1;
+        int be[4] = {0, 0, 0, 0};
+        for (int e1 = 0; e1 < 8; ++e1)
+            for (int e2 = 0; e2 < 8; ++e2)
+                for (int e3 = 0; e3 < 8; ++e3) {
+                    const int off[4] = {0, e1, e2, e3};
+                    long cost = 0;
+                    for (int t = 0; t < 32; ++t)
+                        for (int qw = 0; qw < 4; ++qw) {
+                            int idx[8];
+                            int n = 0;
+                            for (int lane = 8 * qw; lane < 8 * qw + 8; ++lane) {
+                                const int b = t + (lane & (G - 1)) * D;
+                                const int v = off[b & 3] + (b >> 2);
+                                bool seen = false;
+                                for (int i = 0; i < n; ++i) seen = seen || idx[i] == v;
+                                if (!seen) idx[n++] = v;
+                            }
+                            int per[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+                            int worst = 0;
+                            for (int i = 0; i < n; ++i) worst = std::max(worst, ++per[idx[i] & 7]);
+                            cost += worst;
+                        }
+                    if (best < 0 || cost < best) {
+                        best = cost;
+                        be[1] = e1;
+                        be[2] = e2;
+                        be[3] = e3;
+                    }
+                }
+        for (int c = 0; c < 4; ++c) table[B][lg][c] = be[c];
+        done[B][lg] = true;
+    }
+    for (int c = 0; c < 4; ++c) e[c] = table[B][lg][c];
+}
 
 int fill_lane_args(cdtw_handle h, const float* x, int64_t N, const double* mu,
                    const float* sigma, LaneArgs* a) {
@@ -44,6 +105,15 @@ int fill_lane_args(cdtw_handle h, const float* x, int64_t N, const double* mu,
     a->sigma = sigma;
     a->qpad4 = (const float4*)q.qpad;
     a->lq4 = q.lq / 4;
+    // one group per warp (G = 32): the reads of the 32 lanes are all
+    // distinct and shared memory limits the kernel, so the copies take the
+    // bank offsets that spread them; narrower groups read each address twice
+    // or more and keep the copies back to back (measured: the offsets gave
+    // +16 % at W = 409, -2 % at W = 102 and 204)
+    int e[4] = {0, 0, 0, 0};
+    if (G == 32) lane_copy_offsets(B, G, e);
+    const int stride = G == 32 ? lane_copy_stride(q) : a->lq4;
+    for (int c = 0; c < 4; ++c) a->qoff[c] = c * stride + e[c];
     a->qenv = q.env;
     a->M = q.M;
     a->W = q.W;

@@ -49,6 +49,7 @@ struct LaneArgs {
     const float* sigma;
     const float4* qpad4;  // QueryPack::qpad: 4 shifted copies, lq4 float4 each
     int lq4;
+    int qoff[4];          // float4 offset of each copy in the block's shared memory
     const float2* qenv;   // query envelope (search)
     int M, W, G, lgG, Nw;
     int gW, cW;           // lane and slot of band cell k = W
@@ -220,7 +221,7 @@ __device__ __forceinline__ void lane_pair_dtw(const LaneArgs& a, const float4* s
             }
         }
         const int b = t + bstep;
-        const float4* qrow = sq4 + (b & 3) * a.lq4 + (b >> 2);
+        const float4* qrow = sq4 + a.qoff[b & 3] + (b >> 2);
         lane_row<B, EU, KEEP>(p0, p1, z0, z1, qrow, lin0, lin1, r >= 0, last_lane, G);
         lane_raise_slot<B>(p0, p1, a.cph, klim);  // k = 2W+1 stays outside the band
         lin0 = __shfl_up_sync(0xffffffffu, p0[B - 1], 1, G);
@@ -269,9 +270,12 @@ __device__ __forceinline__ void lane_pair_dtw(const LaneArgs& a, const float4* s
     lane_read_slot<B>(p0, p1, a.cW, r0, r1);
 }
 
-// Loads the query copies into shared memory.
+// Loads the query copies into shared memory, copy c at a.qoff[c].
 __device__ __forceinline__ void lane_stage_query(const LaneArgs& a, float4* sq4) {
-    for (int e = threadIdx.x; e < 4 * a.lq4; e += blockDim.x) sq4[e] = a.qpad4[e];
+    for (int e = threadIdx.x; e < 4 * a.lq4; e += blockDim.x) {
+        const int c = e / a.lq4;
+        sq4[a.qoff[c] + (e - c * a.lq4)] = a.qpad4[e];
+    }
     __syncthreads();
 }
 
