@@ -87,6 +87,30 @@ def test_topk_device_equals_host_topk(handle, kind, n, M, P, k, metric):
         np.testing.assert_array_equal(dl, greedy(full, k, M))
 
 
+@pytest.mark.parametrize("variant", ["lane", "strip16", "auto"])
+def test_topk_device_wide_band_variants(handle, variant):
+    """Wide bands (W = 102): the candidates under the threshold are collected
+    by the lane-group or strip search kernels' hit list; the picks equal
+    cdtw_topk's and the greedy over the unpruned all-windows cDTW."""
+    x = synth.metal_like(1 << 17, seed=12)
+    M, W, k = 512, 102, 30
+    q, _ = synth.cut_query(x, M, seed=13, noise=0.2)
+    dx = torch.from_numpy(x).cuda()
+    avg, std = handle.avg_std(dx, M)
+    handle.set_query(q, W)
+    handle.set_band_variant(W, W, variant)
+    try:
+        for metric in (0, 1):
+            hl, hd = handle.topk(dx, avg, std, k, metric=metric)
+            dl, dd = handle.topk_device(dx, avg, std, k, metric=metric)
+            np.testing.assert_array_equal(dl, hl)
+            np.testing.assert_array_equal(dd, hd)
+            full = handle.gpu_cdtw(dx, avg, std, metric=metric).cpu().numpy()
+            np.testing.assert_array_equal(dl, greedy(full, k, M))
+    finally:
+        handle.set_band_variant(W, W, "auto")
+
+
 def test_topk_errors(handle):
     from cudadtw_b200 import CudaDTWError
     x = torch.from_numpy(synth.ecg_like(5000, seed=1)).cuda()
