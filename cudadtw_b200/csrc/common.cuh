@@ -136,9 +136,13 @@ int launch_pair_znorm(cdtw_handle h, const float* q, const float* s, int64_t n, 
 // pairs share the query at zq).  gate: a device count of the pairs present
 // (the first min(n, *gate) run; warps past them exit at once), and the
 // launch does nothing when *gate > gate_max (decisions the host cannot see).
+// gate_min: the launch also does nothing when *gate <= gate_min; wide: (no
+// path record) lane groups of 32 with the fewest cells per lane -- the
+// shortest step, for a handful of pairs.
 int launch_pair_fwd(cdtw_handle h, const float* zq, const float* zs, int64_t n, int L, int W,
                     bool euclid, float* D, uint32_t* dirs, uint32_t* rows, uint32_t* cols,
-                    int64_t qstride = -1, const int* gate = nullptr, int gate_max = 0);
+                    int64_t qstride = -1, const int* gate = nullptr, int gate_max = 0,
+                    int gate_min = -1, bool wide = false);
 // Checkpointed path record (memory: pair_ckpt_floats per pair instead of the
 // direction scratch); pair_ckpt_floats is 0 where the mode does not apply.
 size_t pair_ckpt_floats(int L, int W);

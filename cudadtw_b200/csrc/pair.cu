@@ -302,11 +302,15 @@ int launch_pair_znorm(cdtw_handle h, const float* q, const float* s, int64_t n, 
 
 int launch_pair_fwd(cdtw_handle h, const float* zq, const float* zs, int64_t n, int L, int W,
                     bool euclid, float* D, uint32_t* dirs, uint32_t* rows, uint32_t* cols,
-                    int64_t qstride, const int* gate, int gate_max) {
+                    int64_t qstride, const int* gate, int gate_max, int gate_min,
+                    bool wide) {
     int G, C;
     pair_shape(L, W, &G, &C);
     if (C > 16) return set_error(h, CDTW_EUNSUPPORTED, "pair band W=%d exceeds 511", W);
-    if (!rows && G > 4 && (W + 1 + G / 2 - 1) / (G / 2) <= 8) {
+    if (!rows && wide) {
+        G = 32;
+        C = (W + 1 + G - 1) / G;
+    } else if (!rows && G > 4 && (W + 1 + G / 2 - 1) / (G / 2) <= 8) {
         // distance only (no record whose layout fixes the shape): half as
         // many lanes with twice the cells each -- more independent cells per
         // step for the same dependent chain (measured: the search's seed pass
@@ -320,6 +324,7 @@ int launch_pair_fwd(cdtw_handle h, const float* zq, const float* zs, int64_t n, 
     a.qstride = qstride < 0 ? L : qstride;
     a.gate = gate;
     a.gate_max = gate_max;
+    a.gate_min = gate_min;
     a.n = n;
     a.L = L;
     a.W = W;
@@ -376,6 +381,7 @@ int launch_pair_fwd_ckpt(cdtw_handle h, const float* zq, const float* zs, int64_
     a.qstride = L;
     a.gate = nullptr;
     a.gate_max = 0;
+    a.gate_min = -1;
     a.n = n;
     a.L = L;
     a.W = W;

@@ -48,6 +48,7 @@ struct PairArgs {
     int recb, logb;       // shared-record mode: bytes of record and move log per group
     const int* gate;      // when set: a device count of the pairs present (at most n);
     int gate_max;         // the launch does nothing when it exceeds gate_max
+    int gate_min;         // or when it is at most gate_min
     uint32_t* rows;       // per pair L words: a_i | b_i << 16
     uint32_t* cols;       // per pair L words: c_j | d_j << 16
     float* ckpt;          // checkpointed mode: per pair nseg x 2C x G floats
@@ -486,7 +487,7 @@ __global__ void __launch_bounds__(kPairThreads, 4) pair_fwd_kernel(const PairArg
     int64_t np = a.n;  // pairs present
     if (a.gate) {
         const int c = *a.gate;
-        if (c > a.gate_max) return;  // uniform for the whole launch
+        if (c > a.gate_max || c <= a.gate_min) return;  // uniform for the whole launch
         np = min(np, (int64_t)max(c, 0));
     }
     const int G = a.G, L = a.L, W = a.W;

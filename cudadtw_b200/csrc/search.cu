@@ -55,6 +55,7 @@ constexpr int kSeedMax = 4096;                     // seed_target's upper limit
 constexpr int64_t kSeedZMax = (int64_t)1 << 24;    // floats of seed windows (64 MB)
 constexpr float kSeedBoundSlack = 1.0f + 1e-4f;
 constexpr int kWaveSurvivors = 8192;               // survivors cDTW'd as wavefronts (at most)
+constexpr int kWaveFew = 256;                      // of them, run by the widest lane groups
 constexpr double kWaveMinCells = 4.0e4;            // band cells per window for that
 
 // The seed windows, z-normalised (FP64 arithmetic, rounded once), one row of
@@ -783,8 +784,13 @@ int run_search(cdtw_handle h, const float* x, int64_t N, const double* mu, const
         wave_gather_kernel<<<(unsigned)div_up((int64_t)wcap * 32, 256), 256, 0, h->stream>>>(
             x, mu, sigma, ws.q2, ws.ctr + 1, wcap, q.M, ws.seed_z, ws.ctr + 3);
         CDTW_LAUNCH(h, "wave_gather_kernel");
+        // a handful of survivors: the widest lane groups (shortest step);
+        // more: the throughput shape (each launch gated to its range)
+        CDTW_TRY(launch_pair_fwd(h, q.zq, ws.seed_z, kWaveFew, q.M, Wp, euclid, ws.seed_d,
+                                 nullptr, nullptr, nullptr, /*qstride=*/0, ws.ctr + 1, kWaveFew,
+                                 -1, /*wide=*/true));
         CDTW_TRY(launch_pair_fwd(h, q.zq, ws.seed_z, wcap, q.M, Wp, euclid, ws.seed_d, nullptr,
-                                 nullptr, nullptr, /*qstride=*/0, ws.ctr + 1, wcap));
+                                 nullptr, nullptr, /*qstride=*/0, ws.ctr + 1, wcap, kWaveFew));
         wave_keys_kernel<<<(unsigned)div_up(wcap, 256), 256, 0, h->stream>>>(
             ws.seed_d, ws.q2, ws.ctr + 1, wcap, ws.key);
         CDTW_LAUNCH(h, "wave_keys_kernel");
