@@ -224,20 +224,26 @@ keogh_filter_kernel(const float* __restrict__ x, const double* __restrict__ mu,
         const float* __restrict__ xw = x + w;
         const float2* __restrict__ ew = xenv + w;
         float af = 0.f, ar = 0.f;
-        for (int k0 = 0; k0 < M; k0 += 16) {
-            const int k1 = min(k0 + 16, M);
-            for (int k = k0; k < k1; ++k) {
-                const float z = znorm(nm, __ldg(xw + k));
-                const float2 e = __ldg(qenv + k);
-                const float df = max3f(z - e.y, e.x - z, 0.f);
-                af = EU ? fmaf(df, df, af) : af + df;
-                const float2 d = __ldg(ew + k);
-                const float q = __ldg(zq + k);
-                const float dr = max3f(q - znorm(nm, d.y), znorm(nm, d.x) - q, 0.f);
-                ar = EU ? fmaf(dr, dr, ar) : ar + dr;
-            }
+        auto term = [&](int k) {
+            const float z = znorm(nm, __ldg(xw + k));
+            const float2 e = __ldg(qenv + k);
+            const float df = max3f(z - e.y, e.x - z, 0.f);
+            af = EU ? fmaf(df, df, af) : af + df;
+            const float2 d = __ldg(ew + k);
+            const float q = __ldg(zq + k);
+            const float dr = max3f(q - znorm(nm, d.y), znorm(nm, d.x) - q, 0.f);
+            ar = EU ? fmaf(dr, dr, ar) : ar + dr;
+        };
+        int k0 = 0;
+        // blocks of 16 samples, unrolled so their loads are all in flight
+        // together; a warp-uniform early exit after each block
+        for (; k0 + 16 <= M; k0 += 16) {
+#pragma unroll
+            for (int u = 0; u < 16; ++u) term(k0 + u);
             if (__all_sync(0xffffffffu, !valid || fmaxf(af, ar) >= lim)) break;
         }
+        if (k0 + 16 > M && !__all_sync(0xffffffffu, !valid || fmaxf(af, ar) >= lim))
+            for (int k = k0; k < M; ++k) term(k);
         const float lb = fmaxf(lbkim[w], fmaxf(af, ar));
         const bool keep = valid && lb < lim;
         const unsigned m = __ballot_sync(0xffffffffu, keep);
