@@ -4,14 +4,15 @@
 // Reference: avg_std splits the window statistics into epochs of 1e7 samples
 // (include/stats.cuh:115-142) and UCR_DTW_BIN.cpp:579-707 reads the data in
 // EPOCH-sized chunks, carrying the last m-1 samples into the next chunk and
-// the best-so-far across chunks.  Here the samples the caller pushes fill a
-// pinned staging buffer; each full chunk of C samples is copied to the device
-// on a copy stream, the M-1 samples before it (the halo) are copied from the
-// previous chunk's device buffer, and the chunk's windows are searched on the
+// the best-so-far across chunks.  Here the samples the caller pushes are
+// copied on a copy stream straight into the current device chunk (directly
+// from page-locked memory, else through two pinned staging buffers); when C
+// samples are in, the M-1 samples before them (the halo) are copied from the
+// previous chunk's device buffer and the chunk's windows are searched on the
 // handle's stream starting from the best distance of the earlier chunks (a
-// device-side carried key: no host round trip between chunks).  Two staging
-// and two device buffers alternate, so the copy of one chunk overlaps the
-// search of the previous one.  Windows are numbered globally: chunk k's
+// device-side carried key: no host round trip between chunks).  Two device
+// buffers alternate, so the copies into one chunk overlap the search of the
+// previous one.  Windows are numbered globally: chunk k's
 // windows start at k*C - (M-1) (chunk 0's at 0); ties keep the earliest.
 // The buffers outlive a stream and serve the next one when large enough.
 #include "common.cuh"
@@ -47,6 +48,9 @@ struct StreamState {
     int64_t scap = 0;        // floats per staging buffer
     cudaStream_t copy = nullptr;
     cudaEvent_t staged[2] = {nullptr, nullptr};  // H2D from stage[b] done
+    cudaEvent_t pushed = nullptr;                // a push's copies from page-locked memory
+    int slot = 0;                                // next staging buffer
+    bool slot_used[2] = {false, false};
     cudaEvent_t done[2] = {nullptr, nullptr};    // search over dbuf[b] done
     cudaEvent_t copied[2] = {nullptr, nullptr};  // dbuf[b] filled (halo + chunk)
     bool active = false;     // between begin and end
@@ -62,6 +66,8 @@ struct StreamState {
         fill = chunks = total = 0;
         cur = 0;
         used[0] = used[1] = false;
+        slot = 0;
+        slot_used[0] = slot_used[1] = false;
     }
     void free_stage() {
         for (int b = 0; b < 2; ++b) {
@@ -78,6 +84,7 @@ struct StreamState {
             if (done[b]) cudaEventDestroy(done[b]);
             if (copied[b]) cudaEventDestroy(copied[b]);
         }
+        if (pushed) cudaEventDestroy(pushed);
         if (dmem) cudaFree(dmem);
         if (copy) cudaStreamDestroy(copy);
         *this = StreamState();
@@ -110,24 +117,27 @@ __global__ void stream_merge_kernel(const unsigned long long* __restrict__ key,
 
 StreamState* state(cdtw_handle h) { return reinterpret_cast<StreamState*>(h->stream_state); }
 
-// Copies staging buffer `cur` (n new samples) to the device after the halo,
-// then searches the chunk's windows.
+// Page-locked host memory can be copied to the device directly.
+bool page_locked(const void* p) {
+    cudaPointerAttributes at;
+    if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+        cudaGetLastError();  // plain pageable memory on older drivers
+        return false;
+    }
+    return at.type == cudaMemoryTypeHost;
+}
+
+// Searches the chunk in device buffer `cur`, whose n new samples the pushes
+// have already copied after the halo position: first the halo, the last M-1
+// samples of the previous chunk (at [C, C+M-1) of its buffer), then the
+// chunk's windows.
 int launch_chunk(cdtw_handle h, StreamState& s, int64_t n) {
     const int b = s.cur, o = b ^ 1;
     const int M = s.M;
     float* d = s.dbuf[b];
-    // the device buffer's previous search must be done before it is refilled
-    if (s.used[b]) CDTW_CUDA(h, cudaStreamWaitEvent(s.copy, s.done[b], 0));
-    if (s.chunks > 0) {
-        // halo: the last M-1 samples of the previous chunk (at [C', C'+M-1) of
-        // its buffer, C' its new samples); ordered after that chunk's copy
-        CDTW_CUDA(h, cudaStreamWaitEvent(s.copy, s.copied[o], 0));
+    if (s.chunks > 0)  // after the previous chunk's copies (the same copy stream)
         CDTW_CUDA(h, cudaMemcpyAsync(d, s.dbuf[o] + s.C, sizeof(float) * (M - 1),
                                      cudaMemcpyDeviceToDevice, s.copy));
-    }
-    CDTW_CUDA(h, cudaMemcpyAsync(d + (M - 1), s.stage[b], sizeof(float) * n,
-                                 cudaMemcpyHostToDevice, s.copy));
-    CDTW_CUDA(h, cudaEventRecord(s.staged[b], s.copy));
     CDTW_CUDA(h, cudaEventRecord(s.copied[b], s.copy));
     s.used[b] = true;
     // search: chunk 0 has no halo; later chunks start M-1 samples early
@@ -241,6 +251,8 @@ int cdtw_stream_begin(cdtw_handle h, const float* h_query, int M, int W, int met
             st = check_cuda(h, cudaEventCreateWithFlags(&s->copied[b], cudaEventDisableTiming),
                             "event");
     }
+    if (st == CDTW_OK && !s->pushed)
+        st = check_cuda(h, cudaEventCreateWithFlags(&s->pushed, cudaEventDisableTiming), "event");
     if (st == CDTW_OK && !s->copy)
         st = check_cuda(h, cudaStreamCreateWithFlags(&s->copy, cudaStreamNonBlocking), "stream");
     if (st != CDTW_OK) {
@@ -269,14 +281,36 @@ int cdtw_stream_push(cdtw_handle h, const float* h_samples, int64_t n) {
     StreamState* s = state(h);
     if (!s || !s->active) return set_error(h, CDTW_EINVAL, "no stream begun (cdtw_stream_begin)");
     if (n < 0 || (n > 0 && !h_samples)) return set_error(h, CDTW_EINVAL, "bad samples");
+    if (n == 0) return CDTW_OK;
     CDTW_CUDA(h, cudaSetDevice(h->device));
+    // samples go straight into the current device chunk: from page-locked
+    // memory by one copy (waited for before returning, the caller may reuse
+    // its buffer), else through the two pinned staging buffers in turn
+    const bool pinned = page_locked(h_samples);
     while (n > 0) {
-        if (s->fill == 0 && s->used[s->cur]) {
-            // the staging buffer is free once its last copy has left it
-            CDTW_CUDA(h, cudaEventSynchronize(s->staged[s->cur]));
-        }
+        // a device buffer is refilled after its previous chunk's search
+        if (s->fill == 0 && s->used[s->cur])
+            CDTW_CUDA(h, cudaStreamWaitEvent(s->copy, s->done[s->cur], 0));
         const int64_t take = std::min(n, s->C - s->fill);
-        memcpy(s->stage[s->cur] + s->fill, h_samples, sizeof(float) * take);
+        float* dst = s->dbuf[s->cur] + (s->M - 1) + s->fill;
+        if (pinned) {
+            CDTW_CUDA(h, cudaMemcpyAsync(dst, h_samples, sizeof(float) * take,
+                                         cudaMemcpyHostToDevice, s->copy));
+        } else {
+            for (int64_t a = 0; a < take;) {
+                const int64_t part = std::min(take - a, s->scap);
+                const int sl = s->slot;
+                // a staging buffer is free once its last copy has left it
+                if (s->slot_used[sl]) CDTW_CUDA(h, cudaEventSynchronize(s->staged[sl]));
+                memcpy(s->stage[sl], h_samples + a, sizeof(float) * part);
+                CDTW_CUDA(h, cudaMemcpyAsync(dst + a, s->stage[sl], sizeof(float) * part,
+                                             cudaMemcpyHostToDevice, s->copy));
+                CDTW_CUDA(h, cudaEventRecord(s->staged[sl], s->copy));
+                s->slot_used[sl] = true;
+                s->slot ^= 1;
+                a += part;
+            }
+        }
         s->fill += take;
         s->total += take;
         h_samples += take;
@@ -286,6 +320,10 @@ int cdtw_stream_push(cdtw_handle h, const float* h_samples, int64_t n) {
             s->fill = 0;
             s->cur ^= 1;
         }
+    }
+    if (pinned) {
+        CDTW_CUDA(h, cudaEventRecord(s->pushed, s->copy));
+        CDTW_CUDA(h, cudaEventSynchronize(s->pushed));
     }
     return CDTW_OK;
 }
