@@ -477,12 +477,12 @@ def subresults(h, dev, peak=None) -> dict:
             h.stream_push(xp[a:a + (1 << 22)])
         return h.stream_end()
     streamed()
-    h.search_host(q, x, w)
+    h.search_host(q, xp, w)
     t0 = time.perf_counter()
     sl, sd, _ = streamed()
     ts = time.perf_counter() - t0
     t0 = time.perf_counter()
-    hl, hd = h.search_host(q, x, w)
+    hl, hd = h.search_host(q, xp, w)  # the whole stream in one copy, then the search
     th = time.perf_counter() - t0
     out["stream_search"] = {"stream": "metal 2^25 (host, pinned)", "M": 256, "P": 10, "W": w,
                             "chunk_samples": 1 << 23, "pieces": 8, "streamed_s": ts,
