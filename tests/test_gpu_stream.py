@@ -91,6 +91,24 @@ def test_stream_full_size_metal(handle):
     assert loc == ploc and abs(dist - pdist) <= 1e-5 * pdist
 
 
+def test_stream_from_page_locked_memory(handle):
+    """Pushes from page-locked memory are copied straight into the device
+    chunk (no staging): same result as pushing the same samples from pageable
+    memory, and the caller's buffer may be overwritten as soon as a push
+    returns."""
+    x = synth.ecg_like(500_000, seed=17)
+    q, _ = synth.cut_query(x, 200, seed=4, noise=0.1)
+    ref = _stream_search(handle, q, x, 20, chunk=100_000, seed=2)
+    buf = torch.empty(37_000, dtype=torch.float32).pin_memory().numpy()
+    handle.stream_begin(q, 20, chunk=100_000)
+    for a in range(0, x.size, buf.size):
+        piece = x[a:a + buf.size]
+        buf[:piece.size] = piece
+        handle.stream_push(buf[:piece.size])
+        buf[:] = np.nan  # reused at once: the push has finished with it
+    assert handle.stream_end() == ref
+
+
 def test_stream_buffers_reused_across_streams(handle):
     """Streams back to back on one handle reuse the buffers of the earlier
     ones (growing them for a larger chunk or query); a stream begun again
