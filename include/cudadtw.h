@@ -174,10 +174,12 @@ int cdtw_search_host(cdtw_handle h, const float* h_query, int M, const float* h_
  * pieces of any size and never held whole on the device: the avg_std epochs
  * (include/stats.cuh:115-142) and the EPOCH loop of UCR_DTW_BIN.cpp:579-707,
  * which carries the last m-1 samples and the best-so-far from chunk to
- * chunk.  Samples are staged in chunks of `chunk` samples (0: 2^23); each
- * chunk's copy to the device overlaps the search of the previous one, and
- * every chunk's search starts from the best distance of the chunks before it
- * (kept on the device).  The query (host, M >= 11 floats, band W) stays in
+ * chunk.  The device searches chunks of `chunk` samples (0: 2^23); each push
+ * is copied straight into the current device chunk (from page-locked memory
+ * in one copy, else through pinned staging buffers), the copies overlap the
+ * search of the previous chunk, and every chunk's search starts from the
+ * best distance of the chunks before it (kept on the device).  The caller
+ * may reuse its buffer as soon as cdtw_stream_push returns.  The query (host, M >= 11 floats, band W) stays in
  * the handle until cdtw_stream_end; the handle must not run other searches
  * in between.  Windows are numbered from the first sample pushed (64-bit);
  * ties keep the earliest window, as UCR_DTW_BIN.cpp:682.  cdtw_stream_end
