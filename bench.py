@@ -656,12 +656,15 @@ def profile_case(name: str) -> None:
     dev = torch.device("cuda", 0)
     with Handle(0) as h:
         for _ in range(2):
-            if name == "search":
+            if name in ("search", "search1024"):
+                # config-1 pruned search: M=512, P=10 ("search") or M=1024,
+                # P=20 ("search1024", the widest band)
+                m, p = (512, 10) if name == "search" else (1024, 20)
                 x = synth.metal_like(1 << 25, seed=1)
                 dx = torch.from_numpy(x).to(dev)
-                q, _ = synth.cut_query(x, 512, seed=622, noise=0.1)
-                avg, std = h.avg_std(dx, 512)
-                h.set_query(q, synth.band_from_percent(512, 10))
+                q, _ = synth.cut_query(x, m, seed=100 + m + p, noise=0.1)
+                avg, std = h.avg_std(dx, m)
+                h.set_query(q, synth.band_from_percent(m, p))
                 h.prune_cdtw(dx, avg, std)
             elif name == "topk":
                 x = synth.ecg_like(1 << 22, seed=0)
@@ -740,8 +743,8 @@ def main() -> None:
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--profile",
-                    choices=["search", "topk", "pair", "refine", "refine_search", "strip", "wide",
-                             "wide409", "batch_short"],
+                    choices=["search", "search1024", "topk", "pair", "refine", "refine_search",
+                             "strip", "wide", "wide409", "batch_short"],
                     help="run one small case of that row twice (for ncu) and exit")
     ap.add_argument("--no-sub", action="store_true",
                     help="skip the pruned / batched search and pair fwd/bwd sub-results")
