@@ -115,6 +115,15 @@ __global__ void wave_keys_kernel(const float* __restrict__ d, const Cand* __rest
 // distance as the search kernels compute it lies below this bound (also for
 // an exact match, distance 0): the bound prunes nothing that could be the
 // best, and the best window replaces it in the key.
+__global__ void seed_bound_kernel(const float* __restrict__ d, const Cand* __restrict__ cands,
+                                  int nseed, int M, unsigned long long* __restrict__ key) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool ok = i < nseed && cands[i].lb < CDTW_INF && d[i] == d[i] && d[i] < CDTW_INF;
+    const float b = ok ? d[i] * kSeedBoundSlack + 1e-6f * (float)M : CDTW_INF;
+    const unsigned long long k = warp_min_key(ok, b, 0xffffffffu);
+    if ((threadIdx.x & 31) == 0 && k != ~0ull) atomicMin(key, k);
+}
+
 // The same raising for seeds whose cDTW the search kernels computed into a
 // key of their own (skey: the best seed's packed distance and window).
 __global__ void seed_key_bound_kernel(const unsigned long long* __restrict__ skey, int M,
@@ -126,33 +135,29 @@ __global__ void seed_key_bound_kernel(const unsigned long long* __restrict__ ske
     atomicMin(key, pack_key(d * kSeedBoundSlack + 1e-6f * (float)M, 0xffffffffu));
 }
 
-__global__ void seed_bound_kernel(const float* __restrict__ d, const Cand* __restrict__ cands,
-                                  int nseed, int M, unsigned long long* __restrict__ key) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const bool ok = i < nseed && cands[i].lb < CDTW_INF && d[i] == d[i] && d[i] < CDTW_INF;
-    const float b = ok ? d[i] * kSeedBoundSlack + 1e-6f * (float)M : CDTW_INF;
-    const unsigned long long k = warp_min_key(ok, b, 0xffffffffu);
-    if ((threadIdx.x & 31) == 0 && k != ~0ull) atomicMin(key, k);
-}
-
 // Seed candidates: the smallest-bound window of each group of G blocks; with
 // bmax, the largest LB_Kim of all windows into *kmax (float bits).
 __global__ void seeds_to_cands_kernel(const unsigned long long* __restrict__ seeds,
                                       const unsigned* __restrict__ bmax, int nblk, int G,
                                       Cand* __restrict__ cands, int* __restrict__ nseeds,
                                       unsigned* __restrict__ kmax) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    // a warp per group of G blocks (groups of hundreds of blocks are common)
+    const int lane = threadIdx.x & 31;
+    const int i = (int)(((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
     const int n = (nblk + G - 1) / G;
-    if (i == 0) *nseeds = n;
+    if (i == 0 && lane == 0) *nseeds = n;
+    if (i >= n) return;  // whole warps
     unsigned long long k = ~0ull;
     unsigned mx = 0u;
-    for (int b = i * G; b < min(nblk, (i + 1) * G); ++b) {
+    for (int b = i * G + lane; b < min(nblk, (i + 1) * G); b += 32) {
         k = min(k, seeds[b]);
         if (bmax) mx = max(mx, bmax[b]);
     }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) k = min(k, __shfl_xor_sync(0xffffffffu, k, o));
     mx = __reduce_max_sync(0xffffffffu, mx);
-    if ((threadIdx.x & 31) == 0 && mx) atomicMax(kmax, mx);
-    if (i >= n) return;
+    if (lane != 0) return;
+    if (mx) atomicMax(kmax, mx);
     Cand c;
     c.w = (k == ~0ull) ? 0 : (int)(uint32_t)k;
     c.lb = (k == ~0ull) ? CDTW_INF : 0.f;  // empty block: never started
@@ -377,6 +382,10 @@ keogh_sparse_kernel(const float* __restrict__ x, int64_t N, const double* __rest
 }
 
 constexpr int kSparseSpanMax = 6144;  // M + 2W of the per-window envelope (48 KB a warp)
+// The dense regime (stream envelope + a thread per survivor) was also tried
+// from a per-window work estimate (span x doubling passes): at M=1024, W=102
+// and 204 it measured no faster than the per-window envelopes (586 against
+// 548 us; 1.17 against 0.83 ms per search), so the choice stays by count.
 
 // Forward + reverse LB_Keogh of the LB_Kim survivors q1 (count *n1, known
 // only on the device) into q2 / *n2: up to sparse_max survivors a warp per
@@ -749,7 +758,7 @@ int run_search(cdtw_handle h, const float* x, int64_t N, const double* mu, const
     // 2. cDTW of the seeds
     const int G = (int)std::max<int64_t>(1, div_up(nblk, seed_target(q.M, q.W)));
     const int nseed = (int)div_up(nblk, G);
-    seeds_to_cands_kernel<<<(unsigned)div_up(nseed, 256), 256, 0, h->stream>>>(
+    seeds_to_cands_kernel<<<(unsigned)div_up((int64_t)nseed * 32, 256), 256, 0, h->stream>>>(
         ws.seeds, ws.bmax, (int)nblk, G, ws.seed_cands, ws.ctr + 4, (unsigned*)ws.ctr + 5);
     CDTW_LAUNCH(h, "seeds_to_cands_kernel");
     // the seeds only bound the search from above (raised a little, with no
