@@ -278,9 +278,10 @@ __device__ __forceinline__ float warp_sum_f(float v) {
 // sum passes the best-so-far; then, for the windows still below, the reverse
 // bound against the +-W envelope of the window's own span of the stream,
 // x[w-W, w+M-1+W] clipped to [0, N) (the values env_window_kernel computes
-// for the whole stream), built in shared memory by doubling the min/max spans
-// up to the largest power of two p <= 2W+1.  Survivors -> q2 as in
-// keogh_filter_kernel.  Shared memory: 2 * S floats per warp, S >= M + 2W.
+// for the whole stream), built in shared memory by the van Herk / Gil-Werman
+// split (about five operations per span position at any W; the doubling
+// passes it replaced took log2(2W+1) passes of six).  Survivors -> q2 as in
+// keogh_filter_kernel.  Shared memory: 4 * S floats per warp, S >= M + 2W.
 template <bool EU>
 __global__ void __launch_bounds__(256)
 keogh_sparse_kernel(const float* __restrict__ x, int64_t N, const double* __restrict__ mu,
@@ -294,12 +295,12 @@ keogh_sparse_kernel(const float* __restrict__ x, int64_t N, const double* __rest
     if (n1 > sparse_max) return;  // keogh_filter_kernel takes many survivors
     const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;
-    float* lo = ksm + (size_t)wib * 2 * S;
+    float* lo = ksm + (size_t)wib * 4 * S;
     float* hi = lo + S;
+    float* plo = hi + S;
+    float* phi = plo + S;
     const float lim = load_bsf(key) / kLbSlack;
     const int K = 2 * W + 1, span = M + 2 * W;
-    int p = 1;
-    while (2 * p <= K) p *= 2;
     const int nwarps = (gridDim.x * blockDim.x) >> 5;
     for (int i = (int)(((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5); i < n1;
          i += nwarps) {
@@ -324,9 +325,14 @@ keogh_sparse_kernel(const float* __restrict__ x, int64_t N, const double* __rest
             pruned = tf >= lim;
         }
         if (pruned) continue;
-        // the window's span of the stream, then min/max spans doubled in place
-        // (chunks in increasing order: a partner e + q > e is never rewritten
-        // before it is read)
+        // the window's span of the stream (+inf / -inf outside the stream),
+        // then its +-W envelope by the van Herk / Gil-Werman split: blocks of
+        // K consecutive span positions, extrema from each block start
+        // (prefix, into plo / phi) and to each block end (suffix, in place);
+        // the window [k, k+K) covers the end of one block and the start of
+        // the next: env(k) = ext(suffix[k], prefix[k+K-1]).  A lane scans a
+        // contiguous chunk of CH (odd: conflict-free) positions; the open
+        // block's extremum crosses chunks by a segmented warp scan.
         for (int e = lane; e < span; e += 32) {
             const int64_t g = (int64_t)w - W + e;
             const bool in = g >= 0 && g < N;
@@ -335,22 +341,89 @@ keogh_sparse_kernel(const float* __restrict__ x, int64_t N, const double* __rest
             hi[e] = in ? v : -CDTW_INF;
         }
         __syncwarp();
-        for (int q = 1; q < p; q *= 2) {
-            for (int e0 = 0; e0 < span - q; e0 += 32) {
-                const int e = e0 + lane;
-                float a = 0.f, b = 0.f;
-                if (e < span - q) {
-                    a = fminf(lo[e], lo[e + q]);
-                    b = fmaxf(hi[e], hi[e + q]);
+        const int CH = ((span + 31) / 32) | 1;
+        const int e0 = min(lane * CH, span), e1 = min(e0 + CH, span);
+        {  // prefix extrema within blocks, then the carry from earlier chunks
+            float rl = CDTW_INF, rh = -CDTW_INF;
+            int first = e1;  // first block start in the chunk
+            int r = e0 % K;  // position in the block
+            for (int e = e0; e < e1; ++e) {
+                if (r == 0) {
+                    rl = CDTW_INF;
+                    rh = -CDTW_INF;
+                    first = min(first, e);
                 }
-                __syncwarp();
-                if (e < span - q) {
-                    lo[e] = a;
-                    hi[e] = b;
+                rl = fminf(rl, lo[e]);
+                rh = fmaxf(rh, hi[e]);
+                plo[e] = rl;
+                phi[e] = rh;
+                r = (r == K - 1) ? 0 : r + 1;
+            }
+            bool head = first < e1;  // the scan restarts at a chunk holding a block start
+            float sl = rl, sh = rh;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const float tl = __shfl_up_sync(0xffffffffu, sl, o);
+                const float th = __shfl_up_sync(0xffffffffu, sh, o);
+                const bool tf = __shfl_up_sync(0xffffffffu, head, o);
+                if (lane >= o && !head) {
+                    sl = fminf(sl, tl);
+                    sh = fmaxf(sh, th);
                 }
-                __syncwarp();
+                if (lane >= o) head = head || tf;
+            }
+            float cl = __shfl_up_sync(0xffffffffu, sl, 1);
+            float cr = __shfl_up_sync(0xffffffffu, sh, 1);
+            if (lane == 0) {
+                cl = CDTW_INF;
+                cr = -CDTW_INF;
+            }
+            for (int e = e0; e < first; ++e) {
+                plo[e] = fminf(plo[e], cl);
+                phi[e] = fmaxf(phi[e], cr);
             }
         }
+        {  // suffix extrema within blocks (in place), then the later chunks' carry
+            float rl = CDTW_INF, rh = -CDTW_INF;
+            int last = e0 - 1;  // last block end in the chunk
+            int r = (e1 - 1) % K;
+            for (int e = e1 - 1; e >= e0; --e) {
+                if (r == K - 1 || e == span - 1) {
+                    rl = CDTW_INF;
+                    rh = -CDTW_INF;
+                    last = max(last, e);
+                }
+                rl = fminf(rl, lo[e]);
+                rh = fmaxf(rh, hi[e]);
+                lo[e] = rl;
+                hi[e] = rh;
+                r = (r == 0) ? K - 1 : r - 1;
+            }
+            bool head = last >= e0;
+            float sl = rl, sh = rh;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const float tl = __shfl_down_sync(0xffffffffu, sl, o);
+                const float th = __shfl_down_sync(0xffffffffu, sh, o);
+                const bool tf = __shfl_down_sync(0xffffffffu, head, o);
+                if (lane + o < 32 && !head) {
+                    sl = fminf(sl, tl);
+                    sh = fmaxf(sh, th);
+                }
+                if (lane + o < 32) head = head || tf;
+            }
+            float cl = __shfl_down_sync(0xffffffffu, sl, 1);
+            float cr = __shfl_down_sync(0xffffffffu, sh, 1);
+            if (lane == 31) {
+                cl = CDTW_INF;
+                cr = -CDTW_INF;
+            }
+            for (int e = last + 1; e < e1; ++e) {
+                lo[e] = fminf(lo[e], cl);
+                hi[e] = fmaxf(hi[e], cr);
+            }
+        }
+        __syncwarp();
         // reverse LB_Keogh: the query against the window's envelope
         float ar = 0.f, tr = 0.f;
         for (int k0 = 0; k0 < M && !pruned; k0 += 128) {
@@ -358,8 +431,8 @@ keogh_sparse_kernel(const float* __restrict__ x, int64_t N, const double* __rest
             for (int u = 0; u < 4; ++u) {
                 const int k = k0 + 32 * u + lane;
                 if (k < M) {
-                    const int c = k + K - p;
-                    const float L = fminf(lo[k], lo[c]), U = fmaxf(hi[k], hi[c]);
+                    const int c = k + K - 1;
+                    const float L = fminf(lo[k], plo[c]), U = fmaxf(hi[k], phi[c]);
                     const float qv = __ldg(zq + k);
                     const float dr = max3f(qv - znorm(nm, U), znorm(nm, L) - qv, 0.f);
                     ar = EU ? fmaf(dr, dr, ar) : ar + dr;
@@ -381,7 +454,7 @@ keogh_sparse_kernel(const float* __restrict__ x, int64_t N, const double* __rest
     }
 }
 
-constexpr int kSparseSpanMax = 6144;  // M + 2W of the per-window envelope (48 KB a warp)
+constexpr int kSparseSpanMax = 6144;  // M + 2W of the per-window envelope (96 KB a warp)
 // The dense regime (stream envelope + a thread per survivor) was also tried
 // from a per-window work estimate (span x doubling passes): at M=1024, W=102
 // and 204 it measured no faster than the per-window envelopes (586 against
@@ -414,8 +487,8 @@ int launch_keogh(cdtw_handle h, const float* x, int64_t N, const double* mu, con
     CDTW_LAUNCH(h, "keogh_filter_kernel");
     if (sparse_max <= 0) return CDTW_OK;
     const int wpb = (int)std::max<int64_t>(
-        1, std::min<int64_t>(8, (int64_t)(200 * 1024) / ((int64_t)8 * S)));
-    const size_t smem = (size_t)wpb * 2 * S * sizeof(float);
+        1, std::min<int64_t>(8, (int64_t)(200 * 1024) / ((int64_t)16 * S)));
+    const size_t smem = (size_t)wpb * 4 * S * sizeof(float);
     auto k = euclid ? keogh_sparse_kernel<true> : keogh_sparse_kernel<false>;
     CDTW_CUDA(h, cudaFuncSetAttribute((const void*)k, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)smem));
@@ -794,18 +867,26 @@ int run_search(cdtw_handle h, const float* x, int64_t N, const double* mu, const
     // 5. cDTW of the survivors: as pairwise wavefronts when at most `wcap`
     //    remain and a window is long enough that a thread per window is
     //    latency-bound, else with early abandoning
-    const int wcap = (int)std::min<int64_t>(kWaveSurvivors, ws.seed_cap / q.M);
+    //    When the band runs on the lane-group search kernel (which abandons
+    //    windows early, group by group), only a handful of survivors go to
+    //    the wavefronts: measured at M=1024, W=204, the wavefronts of 4373
+    //    survivors took 0.53 ms.
+    int wcap = (int)std::min<int64_t>(kWaveSurvivors, ws.seed_cap / q.M);
+    if (choose_variant(h, q.W) == CDTW_VARIANT_LANE) wcap = std::min(wcap, kWaveFew);
     if (wave_eligible(q.M, q.W) && wcap >= 32) {
         wave_gather_kernel<<<(unsigned)div_up((int64_t)wcap * 32, 256), 256, 0, h->stream>>>(
             x, mu, sigma, ws.q2, ws.ctr + 1, wcap, q.M, ws.seed_z, ws.ctr + 3);
         CDTW_LAUNCH(h, "wave_gather_kernel");
         // a handful of survivors: the widest lane groups (shortest step);
         // more: the throughput shape (each launch gated to its range)
-        CDTW_TRY(launch_pair_fwd(h, q.zq, ws.seed_z, kWaveFew, q.M, Wp, euclid, ws.seed_d,
-                                 nullptr, nullptr, nullptr, /*qstride=*/0, ws.ctr + 1, kWaveFew,
-                                 -1, /*wide=*/true));
-        CDTW_TRY(launch_pair_fwd(h, q.zq, ws.seed_z, wcap, q.M, Wp, euclid, ws.seed_d, nullptr,
-                                 nullptr, nullptr, /*qstride=*/0, ws.ctr + 1, wcap, kWaveFew));
+        const int few = std::min(wcap, kWaveFew);
+        CDTW_TRY(launch_pair_fwd(h, q.zq, ws.seed_z, few, q.M, Wp, euclid, ws.seed_d, nullptr,
+                                 nullptr, nullptr, /*qstride=*/0, ws.ctr + 1, few, -1,
+                                 /*wide=*/true));
+        if (wcap > few)
+            CDTW_TRY(launch_pair_fwd(h, q.zq, ws.seed_z, wcap, q.M, Wp, euclid, ws.seed_d,
+                                     nullptr, nullptr, nullptr, /*qstride=*/0, ws.ctr + 1, wcap,
+                                     few));
         wave_keys_kernel<<<(unsigned)div_up(wcap, 256), 256, 0, h->stream>>>(
             ws.seed_d, ws.q2, ws.ctr + 1, wcap, ws.key);
         CDTW_LAUNCH(h, "wave_keys_kernel");
