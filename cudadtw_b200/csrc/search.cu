@@ -307,17 +307,24 @@ keogh_sparse_kernel(const float* __restrict__ x, int64_t N, const double* __rest
         const int w = q1[i];
         const Norm nm = make_norm(mu[w], sigma[w]);
         const float* __restrict__ xw = x + w;
-        // forward LB_Keogh, checked every 128 samples
+        // forward LB_Keogh, checked every 256 samples (a lane's eight loads
+        // of the stream and eight of the envelope in flight together)
         float af = 0.f, tf = 0.f;
         bool pruned = false;
-        for (int k0 = 0; k0 < M && !pruned; k0 += 128) {
+        for (int k0 = 0; k0 < M && !pruned; k0 += 256) {
+            float xv[8];
+            float2 ev[8];
 #pragma unroll
-            for (int u = 0; u < 4; ++u) {
-                const int k = k0 + 32 * u + lane;
-                if (k < M) {
-                    const float z = znorm(nm, __ldg(xw + k));
-                    const float2 e = __ldg(qenv + k);
-                    const float df = max3f(z - e.y, e.x - z, 0.f);
+            for (int u = 0; u < 8; ++u) {
+                const int k = min(k0 + 32 * u + lane, M - 1);
+                xv[u] = __ldg(xw + k);
+                ev[u] = __ldg(qenv + k);
+            }
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+                if (k0 + 32 * u + lane < M) {
+                    const float z = znorm(nm, xv[u]);
+                    const float df = max3f(z - ev[u].y, ev[u].x - z, 0.f);
                     af = EU ? fmaf(df, df, af) : af + df;
                 }
             }
@@ -333,12 +340,23 @@ keogh_sparse_kernel(const float* __restrict__ x, int64_t N, const double* __rest
         // the next: env(k) = ext(suffix[k], prefix[k+K-1]).  A lane scans a
         // contiguous chunk of CH (odd: conflict-free) positions; the open
         // block's extremum crosses chunks by a segmented warp scan.
-        for (int e = lane; e < span; e += 32) {
-            const int64_t g = (int64_t)w - W + e;
-            const bool in = g >= 0 && g < N;
-            const float v = in ? __ldg(x + g) : 0.f;
-            lo[e] = in ? v : CDTW_INF;
-            hi[e] = in ? v : -CDTW_INF;
+        for (int s0 = 0; s0 < span; s0 += 256) {
+            float v[8];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+                const int64_t g = (int64_t)w - W + s0 + 32 * u + lane;
+                v[u] = __ldg(x + min(max(g, (int64_t)0), N - 1));
+            }
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+                const int e = s0 + 32 * u + lane;
+                const int64_t g = (int64_t)w - W + e;
+                const bool in = g >= 0 && g < N;
+                if (e < span) {
+                    lo[e] = in ? v[u] : CDTW_INF;
+                    hi[e] = in ? v[u] : -CDTW_INF;
+                }
+            }
         }
         __syncwarp();
         const int CH = ((span + 31) / 32) | 1;
@@ -347,14 +365,13 @@ keogh_sparse_kernel(const float* __restrict__ x, int64_t N, const double* __rest
             float rl = CDTW_INF, rh = -CDTW_INF;
             int first = e1;  // first block start in the chunk
             int r = e0 % K;  // position in the block
+#pragma unroll 4
             for (int e = e0; e < e1; ++e) {
-                if (r == 0) {
-                    rl = CDTW_INF;
-                    rh = -CDTW_INF;
-                    first = min(first, e);
-                }
-                rl = fminf(rl, lo[e]);
-                rh = fmaxf(rh, hi[e]);
+                const bool s = r == 0;
+                const float vl = lo[e], vh = hi[e];
+                rl = fminf(s ? CDTW_INF : rl, vl);
+                rh = fmaxf(s ? -CDTW_INF : rh, vh);
+                if (s) first = min(first, e);
                 plo[e] = rl;
                 phi[e] = rh;
                 r = (r == K - 1) ? 0 : r + 1;
@@ -387,14 +404,13 @@ keogh_sparse_kernel(const float* __restrict__ x, int64_t N, const double* __rest
             float rl = CDTW_INF, rh = -CDTW_INF;
             int last = e0 - 1;  // last block end in the chunk
             int r = (e1 - 1) % K;
+#pragma unroll 4
             for (int e = e1 - 1; e >= e0; --e) {
-                if (r == K - 1 || e == span - 1) {
-                    rl = CDTW_INF;
-                    rh = -CDTW_INF;
-                    last = max(last, e);
-                }
-                rl = fminf(rl, lo[e]);
-                rh = fmaxf(rh, hi[e]);
+                const bool s = r == K - 1 || e == span - 1;
+                const float vl = lo[e], vh = hi[e];
+                rl = fminf(s ? CDTW_INF : rl, vl);
+                rh = fmaxf(s ? -CDTW_INF : rh, vh);
+                if (s) last = max(last, e);
                 lo[e] = rl;
                 hi[e] = rh;
                 r = (r == 0) ? K - 1 : r - 1;
@@ -426,15 +442,17 @@ keogh_sparse_kernel(const float* __restrict__ x, int64_t N, const double* __rest
         __syncwarp();
         // reverse LB_Keogh: the query against the window's envelope
         float ar = 0.f, tr = 0.f;
-        for (int k0 = 0; k0 < M && !pruned; k0 += 128) {
+        for (int k0 = 0; k0 < M && !pruned; k0 += 256) {
+            float qv[8];
 #pragma unroll
-            for (int u = 0; u < 4; ++u) {
+            for (int u = 0; u < 8; ++u) qv[u] = __ldg(zq + min(k0 + 32 * u + lane, M - 1));
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
                 const int k = k0 + 32 * u + lane;
                 if (k < M) {
                     const int c = k + K - 1;
                     const float L = fminf(lo[k], plo[c]), U = fmaxf(hi[k], phi[c]);
-                    const float qv = __ldg(zq + k);
-                    const float dr = max3f(qv - znorm(nm, U), znorm(nm, L) - qv, 0.f);
+                    const float dr = max3f(qv[u] - znorm(nm, U), znorm(nm, L) - qv[u], 0.f);
                     ar = EU ? fmaf(dr, dr, ar) : ar + dr;
                 }
             }
