@@ -278,11 +278,16 @@ __device__ __forceinline__ float warp_sum_f(float v) {
 // sum passes the best-so-far; then, for the windows still below, the reverse
 // bound against the +-W envelope of the window's own span of the stream,
 // x[w-W, w+M-1+W] clipped to [0, N) (the values env_window_kernel computes
-// for the whole stream), built in shared memory by the van Herk / Gil-Werman
-// split (about five operations per span position at any W; the doubling
-// passes it replaced took log2(2W+1) passes of six).  Survivors -> q2 as in
-// keogh_filter_kernel.  Shared memory: 4 * S floats per warp, S >= M + 2W.
-template <bool EU>
+// for the whole stream), built in shared memory.  Survivors -> q2 as in
+// keogh_filter_kernel.  Two ways to the envelope, the same values:
+//  * VH (wide bands): van Herk / Gil-Werman blocks of 2W+1 positions, prefix
+//    and suffix extrema per lane chunk (about five operations per position
+//    at any W); 4 * S floats of shared memory per warp, S >= M + 2W.
+//  * otherwise: log2(2W+1) doubling passes in place; 2 * S floats per warp,
+//    so twice the warps per SM, which wins while the passes are few.
+// Bounds are checked every 128 samples; a lane's loads for 256 are issued
+// together.
+template <bool EU, bool VH>
 __global__ void __launch_bounds__(256)
 keogh_sparse_kernel(const float* __restrict__ x, int64_t N, const double* __restrict__ mu,
                     const float* __restrict__ sigma, const float* __restrict__ zq,
@@ -295,20 +300,21 @@ keogh_sparse_kernel(const float* __restrict__ x, int64_t N, const double* __rest
     if (n1 > sparse_max) return;  // keogh_filter_kernel takes many survivors
     const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;
-    float* lo = ksm + (size_t)wib * 4 * S;
+    float* lo = ksm + (size_t)wib * (VH ? 4 : 2) * S;
     float* hi = lo + S;
-    float* plo = hi + S;
+    float* plo = hi + S;  // VH only
     float* phi = plo + S;
     const float lim = load_bsf(key) / kLbSlack;
     const int K = 2 * W + 1, span = M + 2 * W;
+    int p = 1;  // doubling: the largest power of two <= K
+    while (2 * p <= K) p *= 2;
     const int nwarps = (gridDim.x * blockDim.x) >> 5;
     for (int i = (int)(((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5); i < n1;
          i += nwarps) {
         const int w = q1[i];
         const Norm nm = make_norm(mu[w], sigma[w]);
         const float* __restrict__ xw = x + w;
-        // forward LB_Keogh, checked every 256 samples (a lane's eight loads
-        // of the stream and eight of the envelope in flight together)
+        // forward LB_Keogh
         float af = 0.f, tf = 0.f;
         bool pruned = false;
         for (int k0 = 0; k0 < M && !pruned; k0 += 256) {
@@ -321,25 +327,22 @@ keogh_sparse_kernel(const float* __restrict__ x, int64_t N, const double* __rest
                 ev[u] = __ldg(qenv + k);
             }
 #pragma unroll
-            for (int u = 0; u < 8; ++u) {
-                if (k0 + 32 * u + lane < M) {
-                    const float z = znorm(nm, xv[u]);
-                    const float df = max3f(z - ev[u].y, ev[u].x - z, 0.f);
-                    af = EU ? fmaf(df, df, af) : af + df;
+            for (int h = 0; h < 2; ++h) {
+                if (pruned || k0 + 128 * h >= M) break;  // warp-uniform
+#pragma unroll
+                for (int u = 4 * h; u < 4 * h + 4; ++u) {
+                    if (k0 + 32 * u + lane < M) {
+                        const float z = znorm(nm, xv[u]);
+                        const float df = max3f(z - ev[u].y, ev[u].x - z, 0.f);
+                        af = EU ? fmaf(df, df, af) : af + df;
+                    }
                 }
+                tf = warp_sum_f(af);
+                pruned = tf >= lim;
             }
-            tf = warp_sum_f(af);
-            pruned = tf >= lim;
         }
         if (pruned) continue;
-        // the window's span of the stream (+inf / -inf outside the stream),
-        // then its +-W envelope by the van Herk / Gil-Werman split: blocks of
-        // K consecutive span positions, extrema from each block start
-        // (prefix, into plo / phi) and to each block end (suffix, in place);
-        // the window [k, k+K) covers the end of one block and the start of
-        // the next: env(k) = ext(suffix[k], prefix[k+K-1]).  A lane scans a
-        // contiguous chunk of CH (odd: conflict-free) positions; the open
-        // block's extremum crosses chunks by a segmented warp scan.
+        // the window's span of the stream (+inf / -inf outside the stream)
         for (int s0 = 0; s0 < span; s0 += 256) {
             float v[8];
 #pragma unroll
@@ -359,84 +362,112 @@ keogh_sparse_kernel(const float* __restrict__ x, int64_t N, const double* __rest
             }
         }
         __syncwarp();
-        const int CH = ((span + 31) / 32) | 1;
-        const int e0 = min(lane * CH, span), e1 = min(e0 + CH, span);
-        {  // prefix extrema within blocks, then the carry from earlier chunks
-            float rl = CDTW_INF, rh = -CDTW_INF;
-            int first = e1;  // first block start in the chunk
-            int r = e0 % K;  // position in the block
-#pragma unroll 4
-            for (int e = e0; e < e1; ++e) {
-                const bool s = r == 0;
-                const float vl = lo[e], vh = hi[e];
-                rl = fminf(s ? CDTW_INF : rl, vl);
-                rh = fmaxf(s ? -CDTW_INF : rh, vh);
-                if (s) first = min(first, e);
-                plo[e] = rl;
-                phi[e] = rh;
-                r = (r == K - 1) ? 0 : r + 1;
-            }
-            bool head = first < e1;  // the scan restarts at a chunk holding a block start
-            float sl = rl, sh = rh;
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                const float tl = __shfl_up_sync(0xffffffffu, sl, o);
-                const float th = __shfl_up_sync(0xffffffffu, sh, o);
-                const bool tf = __shfl_up_sync(0xffffffffu, head, o);
-                if (lane >= o && !head) {
-                    sl = fminf(sl, tl);
-                    sh = fmaxf(sh, th);
+        if constexpr (VH) {
+            // blocks of K consecutive span positions: extrema from each block
+            // start (prefix, into plo / phi) and to each block end (suffix, in
+            // place); the window [k, k+K) covers the end of one block and the
+            // start of the next: env(k) = ext(suffix[k], prefix[k+K-1]).  A lane
+            // scans a contiguous chunk of CH (odd: conflict-free) positions;
+            // the open block's extremum crosses chunks by a segmented warp scan.
+            const int CH = ((span + 31) / 32) | 1;
+            const int e0 = min(lane * CH, span), e1 = min(e0 + CH, span);
+            {  // prefix extrema within blocks, then the carry from earlier chunks
+                float rl = CDTW_INF, rh = -CDTW_INF;
+                int first = e1;  // first block start in the chunk
+                int r = e0 % K;  // position in the block
+    #pragma unroll 4
+                for (int e = e0; e < e1; ++e) {
+                    const bool s = r == 0;
+                    const float vl = lo[e], vh = hi[e];
+                    rl = fminf(s ? CDTW_INF : rl, vl);
+                    rh = fmaxf(s ? -CDTW_INF : rh, vh);
+                    if (s) first = min(first, e);
+                    plo[e] = rl;
+                    phi[e] = rh;
+                    r = (r == K - 1) ? 0 : r + 1;
                 }
-                if (lane >= o) head = head || tf;
-            }
-            float cl = __shfl_up_sync(0xffffffffu, sl, 1);
-            float cr = __shfl_up_sync(0xffffffffu, sh, 1);
-            if (lane == 0) {
-                cl = CDTW_INF;
-                cr = -CDTW_INF;
-            }
-            for (int e = e0; e < first; ++e) {
-                plo[e] = fminf(plo[e], cl);
-                phi[e] = fmaxf(phi[e], cr);
-            }
-        }
-        {  // suffix extrema within blocks (in place), then the later chunks' carry
-            float rl = CDTW_INF, rh = -CDTW_INF;
-            int last = e0 - 1;  // last block end in the chunk
-            int r = (e1 - 1) % K;
-#pragma unroll 4
-            for (int e = e1 - 1; e >= e0; --e) {
-                const bool s = r == K - 1 || e == span - 1;
-                const float vl = lo[e], vh = hi[e];
-                rl = fminf(s ? CDTW_INF : rl, vl);
-                rh = fmaxf(s ? -CDTW_INF : rh, vh);
-                if (s) last = max(last, e);
-                lo[e] = rl;
-                hi[e] = rh;
-                r = (r == 0) ? K - 1 : r - 1;
-            }
-            bool head = last >= e0;
-            float sl = rl, sh = rh;
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                const float tl = __shfl_down_sync(0xffffffffu, sl, o);
-                const float th = __shfl_down_sync(0xffffffffu, sh, o);
-                const bool tf = __shfl_down_sync(0xffffffffu, head, o);
-                if (lane + o < 32 && !head) {
-                    sl = fminf(sl, tl);
-                    sh = fmaxf(sh, th);
+                bool head = first < e1;  // the scan restarts at a chunk holding a block start
+                float sl = rl, sh = rh;
+    #pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const float tl = __shfl_up_sync(0xffffffffu, sl, o);
+                    const float th = __shfl_up_sync(0xffffffffu, sh, o);
+                    const bool tf = __shfl_up_sync(0xffffffffu, head, o);
+                    if (lane >= o && !head) {
+                        sl = fminf(sl, tl);
+                        sh = fmaxf(sh, th);
+                    }
+                    if (lane >= o) head = head || tf;
                 }
-                if (lane + o < 32) head = head || tf;
+                float cl = __shfl_up_sync(0xffffffffu, sl, 1);
+                float cr = __shfl_up_sync(0xffffffffu, sh, 1);
+                if (lane == 0) {
+                    cl = CDTW_INF;
+                    cr = -CDTW_INF;
+                }
+                for (int e = e0; e < first; ++e) {
+                    plo[e] = fminf(plo[e], cl);
+                    phi[e] = fmaxf(phi[e], cr);
+                }
             }
-            float cl = __shfl_down_sync(0xffffffffu, sl, 1);
-            float cr = __shfl_down_sync(0xffffffffu, sh, 1);
-            if (lane == 31) {
-                cl = CDTW_INF;
-                cr = -CDTW_INF;
+            {  // suffix extrema within blocks (in place), then the later chunks' carry
+                float rl = CDTW_INF, rh = -CDTW_INF;
+                int last = e0 - 1;  // last block end in the chunk
+                int r = (e1 - 1) % K;
+    #pragma unroll 4
+                for (int e = e1 - 1; e >= e0; --e) {
+                    const bool s = r == K - 1 || e == span - 1;
+                    const float vl = lo[e], vh = hi[e];
+                    rl = fminf(s ? CDTW_INF : rl, vl);
+                    rh = fmaxf(s ? -CDTW_INF : rh, vh);
+                    if (s) last = max(last, e);
+                    lo[e] = rl;
+                    hi[e] = rh;
+                    r = (r == 0) ? K - 1 : r - 1;
+                }
+                bool head = last >= e0;
+                float sl = rl, sh = rh;
+    #pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const float tl = __shfl_down_sync(0xffffffffu, sl, o);
+                    const float th = __shfl_down_sync(0xffffffffu, sh, o);
+                    const bool tf = __shfl_down_sync(0xffffffffu, head, o);
+                    if (lane + o < 32 && !head) {
+                        sl = fminf(sl, tl);
+                        sh = fmaxf(sh, th);
+                    }
+                    if (lane + o < 32) head = head || tf;
+                }
+                float cl = __shfl_down_sync(0xffffffffu, sl, 1);
+                float cr = __shfl_down_sync(0xffffffffu, sh, 1);
+                if (lane == 31) {
+                    cl = CDTW_INF;
+                    cr = -CDTW_INF;
+                }
+                for (int e = last + 1; e < e1; ++e) {
+                    lo[e] = fminf(lo[e], cl);
+                    hi[e] = fmaxf(hi[e], cr);
+                }
             }
-            for (int e = last + 1; e < e1; ++e) {
-                lo[e] = fminf(lo[e], cl);
-                hi[e] = fmaxf(hi[e], cr);
+        } else {
+            // min / max of 2^j positions from e, j = 1.. log2(p), in place
+            // (chunks in increasing order: a partner e + q > e is never
+            // rewritten before it is read)
+            for (int q = 1; q < p; q *= 2) {
+                for (int e0 = 0; e0 < span - q; e0 += 32) {
+                    const int e = e0 + lane;
+                    float a = 0.f, b = 0.f;
+                    if (e < span - q) {
+                        a = fminf(lo[e], lo[e + q]);
+                        b = fmaxf(hi[e], hi[e + q]);
+                    }
+                    __syncwarp();
+                    if (e < span - q) {
+                        lo[e] = a;
+                        hi[e] = b;
+                    }
+                    __syncwarp();
+                }
             }
         }
         __syncwarp();
@@ -447,17 +478,28 @@ keogh_sparse_kernel(const float* __restrict__ x, int64_t N, const double* __rest
 #pragma unroll
             for (int u = 0; u < 8; ++u) qv[u] = __ldg(zq + min(k0 + 32 * u + lane, M - 1));
 #pragma unroll
-            for (int u = 0; u < 8; ++u) {
-                const int k = k0 + 32 * u + lane;
-                if (k < M) {
-                    const int c = k + K - 1;
-                    const float L = fminf(lo[k], plo[c]), U = fmaxf(hi[k], phi[c]);
-                    const float dr = max3f(qv[u] - znorm(nm, U), znorm(nm, L) - qv[u], 0.f);
-                    ar = EU ? fmaf(dr, dr, ar) : ar + dr;
+            for (int h = 0; h < 2; ++h) {
+                if (pruned || k0 + 128 * h >= M) break;  // warp-uniform
+#pragma unroll
+                for (int u = 4 * h; u < 4 * h + 4; ++u) {
+                    const int k = k0 + 32 * u + lane;
+                    if (k < M) {
+                        float L, U;
+                        if constexpr (VH) {
+                            L = fminf(lo[k], plo[k + K - 1]);
+                            U = fmaxf(hi[k], phi[k + K - 1]);
+                        } else {
+                            L = fminf(lo[k], lo[k + K - p]);
+                            U = fmaxf(hi[k], hi[k + K - p]);
+                        }
+                        const float dr =
+                            max3f(qv[u] - znorm(nm, U), znorm(nm, L) - qv[u], 0.f);
+                        ar = EU ? fmaf(dr, dr, ar) : ar + dr;
+                    }
                 }
+                tr = warp_sum_f(ar);
+                pruned = tr >= lim;
             }
-            tr = warp_sum_f(ar);
-            pruned = tr >= lim;
         }
         __syncwarp();  // the span buffer is rewritten for the next window
         if (pruned) continue;
@@ -473,6 +515,7 @@ keogh_sparse_kernel(const float* __restrict__ x, int64_t N, const double* __rest
 }
 
 constexpr int kSparseSpanMax = 6144;  // M + 2W of the per-window envelope (96 KB a warp)
+constexpr int kSparseVHMinBand = 201;  // 2W+1 from which the van Herk blocks serve it
 // The dense regime (stream envelope + a thread per survivor) was also tried
 // from a per-window work estimate (span x doubling passes): at M=1024, W=102
 // and 204 it measured no faster than the per-window envelopes (586 against
@@ -504,10 +547,16 @@ int launch_keogh(cdtw_handle h, const float* x, int64_t N, const double* mu, con
             ws.ctr + 1, sparse_max);
     CDTW_LAUNCH(h, "keogh_filter_kernel");
     if (sparse_max <= 0) return CDTW_OK;
+    // van Herk blocks from kSparseVHMinBand (measured: doubling faster at
+    // W <= 51 — 39 against 65 us at M=512 — van Herk at W >= 204, and at
+    // M=512, W=102)
+    const bool vh = 2 * W + 1 >= kSparseVHMinBand;
+    const int per_warp = (vh ? 4 : 2) * S;  // floats
     const int wpb = (int)std::max<int64_t>(
-        1, std::min<int64_t>(8, (int64_t)(200 * 1024) / ((int64_t)16 * S)));
-    const size_t smem = (size_t)wpb * 4 * S * sizeof(float);
-    auto k = euclid ? keogh_sparse_kernel<true> : keogh_sparse_kernel<false>;
+        1, std::min<int64_t>(8, (int64_t)(200 * 1024) / ((int64_t)4 * per_warp)));
+    const size_t smem = (size_t)wpb * per_warp * sizeof(float);
+    auto k = vh ? (euclid ? keogh_sparse_kernel<true, true> : keogh_sparse_kernel<false, true>)
+                : (euclid ? keogh_sparse_kernel<true, false> : keogh_sparse_kernel<false, false>);
     CDTW_CUDA(h, cudaFuncSetAttribute((const void*)k, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)smem));
     int per_sm = 0;

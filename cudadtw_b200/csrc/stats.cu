@@ -118,9 +118,11 @@ avg_std_kernel(const XT* __restrict__ x, int64_t N, int M, double* __restrict__ 
 // One block prepares the query pack: FP64 two-pass z-normalisation (the
 // reference does this on the host in FP32, GPU-dtw.cu:67 / stats.cuh:8-28),
 // the +inf-padded shifted copies read by the cDTW kernels, and the +-W
-// envelope (same values as Lemire's filter, bounds.cuh:13-64).
+// envelope (same values as Lemire's filter, bounds.cuh:13-64).  Shared
+// memory: M doubles (zs) and M floats behind them.
 __device__ __forceinline__ void prepare_query_body(const float* __restrict__ qraw, int M, int W,
                                                    const QueryPack& p, double* zs) {
+    float* zf = reinterpret_cast<float*>(zs + M);  // the z-values rounded to float
     __shared__ double red[2][8];
     const int t = threadIdx.x, lane = t & 31, wid = t >> 5;
     double s = 0.0;
@@ -153,6 +155,7 @@ __device__ __forceinline__ void prepare_query_body(const float* __restrict__ qra
     for (int i = t; i < M; i += blockDim.x) {
         const double z = (zs[i] - mean) / sd;
         zs[i] = z;
+        zf[i] = (float)z;
         p.zq64[i] = z;
         p.zq[i] = (float)z;
     }
@@ -176,21 +179,34 @@ __device__ __forceinline__ void prepare_query_body(const float* __restrict__ qra
             p.qrev[e] = v;
         }
     }
-    // envelope over [k-W, k+W] clipped to the query
+    // envelope over [k-W, k+W] clipped to the query, from the float values
+    // (rounding is monotone: the extrema of the rounded values are the
+    // rounded extrema); four independent min / max chains per window
     for (int k = t; k < M; k += blockDim.x) {
-        double lo = zs[k], hi = zs[k];
         const int a0 = max(0, k - W), a1 = min(M - 1, k + W);
-        for (int i = a0; i <= a1; ++i) {
-            lo = fmin(lo, zs[i]);
-            hi = fmax(hi, zs[i]);
+        float lo[4], hi[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) lo[u] = hi[u] = zf[k];
+        int i = a0;
+        for (; i + 3 <= a1; i += 4) {
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                lo[u] = fminf(lo[u], zf[i + u]);
+                hi[u] = fmaxf(hi[u], zf[i + u]);
+            }
         }
-        p.env[k] = make_float2((float)lo, (float)hi);
+        for (; i <= a1; ++i) {
+            lo[0] = fminf(lo[0], zf[i]);
+            hi[0] = fmaxf(hi[0], zf[i]);
+        }
+        p.env[k] = make_float2(fminf(fminf(lo[0], lo[1]), fminf(lo[2], lo[3])),
+                               fmaxf(fmaxf(hi[0], hi[1]), fmaxf(hi[2], hi[3])));
     }
 }
 
 __global__ void __launch_bounds__(256)
 prepare_query_kernel(const float* __restrict__ qraw, int M, int W, QueryPack p) {
-    extern __shared__ double zs[];  // M doubles
+    extern __shared__ double zs[];  // M doubles, M floats
     prepare_query_body(qraw, M, W, p, zs);
 }
 
@@ -232,7 +248,7 @@ int launch_avg_std64(cdtw_handle h, const double* x, int64_t N, int M, double* m
 
 int launch_prepare_queries(cdtw_handle h, const float* raw, const int64_t* offs,
                            const QueryPack* packs, int nq, int max_m) {
-    const size_t smem = (size_t)max_m * sizeof(double);
+    const size_t smem = (size_t)max_m * (sizeof(double) + sizeof(float));
     if (smem > 48 * 1024)
         CDTW_CUDA(h, cudaFuncSetAttribute((const void*)prepare_queries_kernel,
                                           cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -243,7 +259,7 @@ int launch_prepare_queries(cdtw_handle h, const float* raw, const int64_t* offs,
 }
 
 int launch_prepare_query(cdtw_handle h, const float* d_query_raw, int M, int W) {
-    const size_t smem = (size_t)M * sizeof(double);
+    const size_t smem = (size_t)M * (sizeof(double) + sizeof(float));
     if (smem > 48 * 1024)
         CDTW_CUDA(h, cudaFuncSetAttribute((const void*)prepare_query_kernel,
                                           cudaFuncAttributeMaxDynamicSharedMemorySize,
