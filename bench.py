@@ -318,7 +318,8 @@ def subresults(h, dev, peak=None) -> dict:
 
     * pruned_search: config 0 (2^20 ECG-like, M=128, W=12) and config 1
       (2^25 metal-like, M in {128,256,512,1024} x P in {5,10,20}): device time
-      of one full search (statistics excluded; they are shared per M), stream
+      of a full search, the median of five (statistics excluded; they are
+      shared per M), stream
       samples/s, the pruning-inclusive rate windows * cells(M,W) / time, the
       FP64 oracle's distance at the reported window and the relative error,
       and, on the same inputs, the location and wall time of the reference's
@@ -348,6 +349,15 @@ def subresults(h, dev, peak=None) -> dict:
         torch.cuda.synchronize()
         return e0.elapsed_time(e1) / 1e3 / reps, r
 
+    def dev_time_median(fn, n=5):
+        # n single runs, each bracketed by its own events: a host stall
+        # between launches inflates one run, not the median
+        ts, r = [], None
+        for _ in range(n):
+            t, r = dev_time(fn)
+            ts.append(t)
+        return float(np.median(ts)), r
+
     # -- pruned search -----------------------------------------------------
     import oracle
     rows = []
@@ -364,7 +374,7 @@ def subresults(h, dev, peak=None) -> dict:
             avg, std = h.avg_std(dx, m)
             h.set_query(q, w)
             h.prune_cdtw(dx, avg, std)  # warm
-            t, (loc, dist) = dev_time(lambda: h.prune_cdtw(dx, avg, std))
+            t, (loc, dist) = dev_time_median(lambda: h.prune_cdtw(dx, avg, std))
             nwin = x.size - m + 1
             ref = float(np.sqrt(oracle.cdtw_list(q, x, w, np.array([loc]))[0]))
             row = {"case": name, "M": m, "P": pct, "W": w, "ms": t * 1e3,
@@ -553,7 +563,7 @@ def subresults(h, dev, peak=None) -> dict:
     for W in (102, 204, 409):
         h.set_query(q, W)
         h.gpu_cdtw(dx, avg, std)  # warm-up
-        t, _ = dev_time(lambda: h.gpu_cdtw(dx, avg, std), reps=3)
+        t, _ = dev_time_median(lambda: h.gpu_cdtw(dx, avg, std))
         g = (1 << 18) * cells(1024, W) / t / 1e9
         wide[f"W{W}"] = {"ms": t * 1e3, "gcups": g, "variant": "lane group",
                          "frac_of_measured_cell_rate": g / (peak / 1e9) if peak else None}
