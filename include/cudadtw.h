@@ -31,7 +31,8 @@ enum cdtw_status {
     CDTW_EINVAL = 1,       /* bad argument (sizes, band, null pointer)            */
     CDTW_ENOMEM = 2,       /* device or pinned host allocation failed             */
     CDTW_ECUDA = 3,        /* a CUDA runtime call or kernel launch failed         */
-    CDTW_ETIMEOUT = 4,     /* a bounded device-side wait gave up                  */
+    CDTW_ETIMEOUT = 4,     /* reserved: no entry point waits on the device for    */
+                           /* another party, so none returns it                   */
     CDTW_EUNSUPPORTED = 5  /* valid request outside what this build implements     */
 };
 
