@@ -272,6 +272,8 @@ __device__ __forceinline__ float warp_sum_f(float v) {
     return v;
 }
 
+constexpr int kSparseMaxWarps = 16;  // warps per block of keogh_sparse_kernel (at most)
+
 // Forward + reverse LB_Keogh for few LB_Kim survivors (at most sparse_max,
 // scattered over the stream): a warp per window, lanes over the window's
 // samples (coalesced).  The forward bound first, abandoned once its running
@@ -288,7 +290,7 @@ __device__ __forceinline__ float warp_sum_f(float v) {
 // Bounds are checked every 128 samples; a lane's loads for 256 are issued
 // together.
 template <bool EU, bool VH>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(32 * kSparseMaxWarps, 1)
 keogh_sparse_kernel(const float* __restrict__ x, int64_t N, const double* __restrict__ mu,
                     const float* __restrict__ sigma, const float* __restrict__ zq,
                     const float2* __restrict__ qenv, const float* __restrict__ lbkim, int M, int W,
@@ -551,12 +553,40 @@ int launch_keogh(cdtw_handle h, const float* x, int64_t N, const double* mu, con
     // W <= 51 — 39 against 65 us at M=512 — van Herk at W >= 204, and at
     // M=512, W=102)
     const bool vh = 2 * W + 1 >= kSparseVHMinBand;
-    const int per_warp = (vh ? 4 : 2) * S;  // floats
-    const int wpb = (int)std::max<int64_t>(
-        1, std::min<int64_t>(8, (int64_t)(200 * 1024) / ((int64_t)4 * per_warp)));
-    const size_t smem = (size_t)wpb * per_warp * sizeof(float);
+    const int64_t per_warp = (int64_t)(vh ? 4 : 2) * S * sizeof(float);  // bytes
     auto k = vh ? (euclid ? keogh_sparse_kernel<true, true> : keogh_sparse_kernel<false, true>)
                 : (euclid ? keogh_sparse_kernel<true, false> : keogh_sparse_kernel<false, false>);
+    // warps per block for the most warps per SM: shared memory per SM and per
+    // block (less the per-block reservation), registers, the warp limit
+    int smem_sm = 0, smem_blk = 0, resv = 0, warps_sm = 0, blocks_sm = 0;
+    CDTW_CUDA(h, cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor,
+                                        h->device));
+    CDTW_CUDA(h, cudaDeviceGetAttribute(&smem_blk, cudaDevAttrMaxSharedMemoryPerBlockOptin,
+                                        h->device));
+    CDTW_CUDA(h, cudaDeviceGetAttribute(&resv, cudaDevAttrReservedSharedMemoryPerBlock,
+                                        h->device));
+    CDTW_CUDA(h, cudaDeviceGetAttribute(&warps_sm, cudaDevAttrMaxThreadsPerMultiProcessor,
+                                        h->device));
+    CDTW_CUDA(h, cudaDeviceGetAttribute(&blocks_sm, cudaDevAttrMaxBlocksPerMultiprocessor,
+                                        h->device));
+    warps_sm /= 32;
+    cudaFuncAttributes fa;
+    CDTW_CUDA(h, cudaFuncGetAttributes(&fa, (const void*)k));
+    const int64_t regs_warp = (int64_t)((fa.numRegs + 7) / 8 * 8) * 32;
+    const int64_t reg_warps = regs_warp > 0 ? 65536 / regs_warp : warps_sm;
+    int wpb = 1;
+    int64_t best = 0;
+    for (int c = 1; c <= kSparseMaxWarps; ++c) {
+        if (c * per_warp > smem_blk) break;
+        const int64_t nb = std::min<int64_t>(
+            std::min<int64_t>(smem_sm / (c * per_warp + resv), blocks_sm),
+            std::min<int64_t>(warps_sm, reg_warps) / c);
+        if (nb * c >= best) {  // ties: the larger block
+            best = nb * c;
+            wpb = c;
+        }
+    }
+    const size_t smem = (size_t)wpb * per_warp;
     CDTW_CUDA(h, cudaFuncSetAttribute((const void*)k, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)smem));
     int per_sm = 0;
