@@ -205,15 +205,40 @@ __device__ __forceinline__ void lane_pair_dtw(const LaneArgs& a, const float4* s
     const float klim = last_lane ? CDTW_INF : -CDTW_INF;
     const int t_end = M - 1 + a.gW;
     const int bstep = g * (B - 1);
+    // search: the samples of the next step's row (and lane 0's envelope
+    // value of row t+1) are loaded one step ahead, the best-so-far
+    // kLaneCheck / 2 steps before its check: the last survivors of a search
+    // run nearly alone on their SMs and otherwise wait on these loads at every
+    // step (all windows: enough warps hide them, and the extra work cost 7 %)
+    float cx0 = 0.f, cx1 = 0.f, bsf_pf = CDTW_INF;
+    float2 ce = make_float2(0.f, 0.f);
+    if constexpr (SEARCH) {
+        cx0 = __ldg(xw0 + min(max(-g, 0), M - 1));
+        cx1 = __ldg(xw1 + min(max(-g, 0), M - 1));
+        ce = __ldg(a.qenv);
+    }
     auto step = [&](int t, auto keep_tag) {
         constexpr bool KEEP = decltype(keep_tag)::value;
         const int r = t - g;
-        const int rc = min(max(r, 0), M - 1);
-        const float z0 = znorm(n0, __ldg(xw0 + rc));
-        const float z1 = znorm(n1, __ldg(xw1 + rc));
+        float x0, x1;
+        if constexpr (SEARCH) {
+            x0 = cx0;
+            x1 = cx1;
+            const int rn = min(max(r + 1, 0), M - 1);
+            cx0 = __ldg(xw0 + rn);
+            cx1 = __ldg(xw1 + rn);
+        } else {
+            const int rc = min(max(r, 0), M - 1);
+            x0 = __ldg(xw0 + rc);
+            x1 = __ldg(xw1 + rc);
+        }
+        const float z0 = znorm(n0, x0);
+        const float z1 = znorm(n1, x1);
         if constexpr (SEARCH) {  // lane 0's row t: its forward LB_Keogh term
+            const float2 e = ce;
+            ce = __ldg(a.qenv + min(t + 1, M - 1));
+            if ((t & (kLaneCheck - 1)) == kLaneCheck / 2 - 1) bsf_pf = load_bsf(a.key);
             if (t < M) {
-                const float2 e = __ldg(a.qenv + min(t, M - 1));
                 const float d0 = max3f(z0 - e.y, e.x - z0, 0.f);
                 const float d1 = max3f(z1 - e.y, e.x - z1, 0.f);
                 pre0 += EU ? d0 * d0 : d0;
@@ -254,7 +279,7 @@ __device__ __forceinline__ void lane_pair_dtw(const LaneArgs& a, const float4* s
                 }
                 const float q0 = __shfl_sync(0xffffffffu, pre0, 0, G);
                 const float q1 = __shfl_sync(0xffffffffu, pre1, 0, G);
-                const float bsf = load_bsf(a.key);
+                const float bsf = bsf_pf;  // read kLaneCheck / 2 steps ago: at most larger
                 alive0 = alive0 && (m0 + lb_suffix(lbk0, q0, M) * kLbSlack < bsf);
                 alive1 = alive1 && (m1 + lb_suffix(lbk1, q1, M) * kLbSlack < bsf);
                 if (!__any_sync(0xffffffffu, alive0 || alive1)) {
