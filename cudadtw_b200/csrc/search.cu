@@ -517,7 +517,7 @@ keogh_sparse_kernel(const float* __restrict__ x, int64_t N, const double* __rest
 }
 
 constexpr int kSparseSpanMax = 6144;  // M + 2W of the per-window envelope (96 KB a warp)
-constexpr int kSparseVHMinBand = 201;  // 2W+1 from which the van Herk blocks serve it
+constexpr int kSparseVHMinBand = 301;  // 2W+1 from which the van Herk blocks serve it
 // The dense regime (stream envelope + a thread per survivor) was also tried
 // from a per-window work estimate (span x doubling passes): at M=1024, W=102
 // and 204 it measured no faster than the per-window envelopes (586 against
@@ -549,9 +549,10 @@ int launch_keogh(cdtw_handle h, const float* x, int64_t N, const double* mu, con
             ws.ctr + 1, sparse_max);
     CDTW_LAUNCH(h, "keogh_filter_kernel");
     if (sparse_max <= 0) return CDTW_OK;
-    // van Herk blocks from kSparseVHMinBand (measured: doubling faster at
-    // W <= 51 — 39 against 65 us at M=512 — van Herk at W >= 204, and at
-    // M=512, W=102)
+    // van Herk blocks from kSparseVHMinBand (measured: the doubling passes
+    // are faster at W <= 51 — 39 against 65 us at M=512 — and, with the
+    // blocks sized below, at W = 102 — the M=1024 search 0.754 against
+    // 0.787 ms, M=512 the same; van Herk is faster at W = 204)
     const bool vh = 2 * W + 1 >= kSparseVHMinBand;
     const int64_t per_warp = (int64_t)(vh ? 4 : 2) * S * sizeof(float);  // bytes
     auto k = vh ? (euclid ? keogh_sparse_kernel<true, true> : keogh_sparse_kernel<false, true>)
